@@ -1,0 +1,283 @@
+/*
+ * meshtrex-b200 C ABI: the isosurface-extraction path of meshtrex (block
+ * min/max -> active-block filtering + compaction -> PMB marching cubes) on
+ * one NVIDIA B200, behind plain C entry points.
+ *
+ * These calls replace, for compute only, what meshtrex does through its
+ * Vulkan runtime (src/vulkan_context.*, src/device.*, src/buffer.*,
+ * src/image.*) and its three stage managers.  Each declaration names the
+ * meshtrex interface it stands in for.  The C++ drop-in facade with the
+ * reference's own names (computeMinMaxMip, filterActiveBlocks,
+ * readActiveBlockCount, extractMeshletDescriptors) is in the other headers
+ * of this directory and is written on top of this ABI.
+ *
+ * Conventions
+ *  - Every entry point returns mtx_status and never throws or aborts.
+ *  - Pointers named "device" are CUDA device pointers on the context's
+ *    device; everything else is host memory.
+ *  - Work is issued on the context's stream (mtx_context_set_stream, the
+ *    analogue of meshtrex's externalCmd command buffer).  Calls that need a
+ *    host value from the GPU (counts) synchronise that stream; the *_async
+ *    calls never do and can be captured in a CUDA graph.
+ *  - Volumes are x fastest, then y, then z: voxel (x,y,z) is element
+ *    z*X*Y + y*X + x (src/volume.h:8-12, src/testMinMax.h:97-101).
+ */
+#ifndef MESHTREX_MTX_H
+#define MESHTREX_MTX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MTX_ABI_VERSION 1
+#define MTX_MAX_MIP_LEVELS 32
+#define MTX_MAX_BLOCK_EDGE 16
+
+typedef enum mtx_status {
+    MTX_OK = 0,
+    MTX_ERR_INVALID_ARG = 1, /* bad pointer, size, dims or option */
+    MTX_ERR_UNSUPPORTED = 2, /* valid but not implemented (e.g. block edge > 16) */
+    MTX_ERR_OOM = 3,         /* a device or host allocation failed */
+    MTX_ERR_CAPACITY = 4,    /* caller buffers too small; counters hold the needed sizes */
+    MTX_ERR_TIMEOUT = 5,     /* a bounded device-side wait gave up (error word set) */
+    MTX_ERR_CUDA = 6,        /* a CUDA runtime call failed */
+    MTX_ERR_NO_DEVICE = 7,   /* no usable CUDA device */
+    MTX_ERR_INTERNAL = 8     /* an invariant check inside a kernel failed */
+} mtx_status;
+
+typedef enum mtx_dtype {
+    MTX_DTYPE_U8 = 0,  /* meshtrex's only type on the GPU (R8_UINT, minMaxManager.cpp:117) */
+    MTX_DTYPE_U16 = 1, /* loadVolume's 2-byte type (volume.h:29-30) */
+    MTX_DTYPE_F32 = 2
+} mtx_dtype;
+
+/* PushConstants (src/common.h:29-34): same fields, order and 16-byte
+ * alignment.  blockGridDim = ceil(volumeDim / blockDim) (src/meshtrex.cpp:79-83). */
+typedef struct mtx_push_constants {
+    uint32_t volumeDim[4];
+    uint32_t blockDim[4];
+    uint32_t blockGridDim[4];
+    float isovalue;
+    uint32_t _pad[3];
+} mtx_push_constants;
+
+/* A span of device memory: meshtrex's Buffer (src/resources.h, buffer.h:10-18)
+ * reduced to what compute needs. */
+typedef struct mtx_buffer {
+    void *ptr;
+    uint64_t size; /* bytes */
+} mtx_buffer;
+
+typedef struct mtx_context *mtx_context_t;
+typedef struct mtx_profiler *mtx_profiler_t;
+
+/* Device-resident scalar volume: meshtrex's Volume (src/volume.h:8-12) once
+ * uploaded (MinMaxOutput::volumeImage, src/minMaxOutput.h:11). */
+typedef struct mtx_volume {
+    mtx_buffer data;
+    uint32_t dims[3];
+    uint32_t dtype; /* mtx_dtype */
+    uint32_t owned; /* 1 if mtx_volume_free releases data.ptr */
+    uint32_t _pad;
+} mtx_volume;
+
+/* MinMaxOutput (src/minMaxOutput.h:10-65).  minMaxImage holds every mip
+ * level back to back as {min,max} uint32 keys (R32G32_UINT in meshtrex);
+ * levelOffset/levelExtent play the part of minMaxMipViews.  Keys are the
+ * voxel values for u8/u16 and an order-preserving transform for f32
+ * (mtx_key_to_float). */
+typedef struct mtx_minmax_output {
+    mtx_volume volumeImage; /* borrowed copy of the input descriptor */
+    mtx_buffer minMaxImage;
+    uint32_t mipLevels;
+    uint32_t blockDim[3];
+    uint32_t blockGridDim[3];
+    uint32_t levelExtent[MTX_MAX_MIP_LEVELS][3];
+    uint64_t levelOffset[MTX_MAX_MIP_LEVELS]; /* in texels (8 bytes each) */
+} mtx_minmax_output;
+
+/* FilteringOutput (src/filteringOutput.h:11-74) plus the dense rank map the
+ * extraction uses to find a neighbouring block's vertices. */
+typedef struct mtx_filtering_output {
+    mtx_buffer compactedBlockIdBuffer; /* uint32[totalBlocks]; the first count are valid, ascending */
+    mtx_buffer activeBlockCountBuffer; /* uint32 */
+    mtx_buffer blockRankBuffer;        /* uint32[totalBlocks]; rank of block id b, valid where b is active */
+    uint32_t activeBlockCount;         /* host copy: 0 until mtx_read_active_block_count */
+    uint32_t totalBlocks;
+    float isovalue;
+    uint32_t _pad;
+} mtx_filtering_output;
+
+typedef enum mtx_vertex_format {
+    MTX_VERTEX_XYZ = 0, /* 12 bytes: float x, y, z */
+    MTX_VERTEX_DATA = 1 /* 32 bytes: VertexData{vec4 position; vec4 normal} (extractionOutput.h:131-134) */
+} mtx_vertex_format;
+
+typedef enum mtx_frame {
+    MTX_FRAME_VOXEL = 0, /* positions in voxel units (the exact parity frame) */
+    MTX_FRAME_NDC = 1    /* (pos / volumeDim) * 2 - 1, as meshtrex writes (marching_cubes_pmb.mesh.glsl:138) */
+} mtx_frame;
+
+typedef enum mtx_staging {
+    MTX_STAGING_AUTO = 0, /* TMA when the volume's layout allows it */
+    MTX_STAGING_TMA = 1,  /* cp.async.bulk.tensor 3D tile of the block + halo */
+    MTX_STAGING_LDG = 2   /* plain coalesced loads */
+} mtx_staging;
+
+typedef struct mtx_extract_options {
+    uint32_t vertexFormat; /* mtx_vertex_format */
+    uint32_t frame;        /* mtx_frame */
+    uint32_t normals;      /* MTX_VERTEX_DATA only: 1 = fill the normal (pmb.mesh.glsl:111-137) */
+    uint32_t staging;      /* mtx_staging */
+    uint32_t threads;      /* threads per CTA of the extraction kernels; 0 = auto */
+    uint32_t _pad;
+    uint8_t *cellCases;    /* optional device output: B^3 case bytes per active block, rank order */
+} mtx_extract_options;
+
+/* MeshletDescriptor (extractionOutput.h:124-129).  One per active block, in
+ * rank order: its own vertices and its triangles (indexOffset counts uint32s). */
+typedef struct mtx_meshlet_descriptor {
+    uint32_t vertexOffset;
+    uint32_t indexOffset;
+    uint32_t vertexCount;
+    uint32_t primitiveCount;
+} mtx_meshlet_descriptor;
+
+/* ExtractionOutput (src/extractionOutput.h:10-122).  Buffers are sized
+ * exactly, not for the worst case; meshletCount is the true count. */
+typedef struct mtx_extraction_output {
+    mtx_buffer vertexBuffer;
+    mtx_buffer vertexCountBuffer; /* uint32 */
+    mtx_buffer indexBuffer;       /* uint32, 3 per triangle, global vertex ids */
+    mtx_buffer indexCountBuffer;  /* uint32 */
+    mtx_buffer meshletDescriptorBuffer;
+    mtx_buffer meshletDescriptorCountBuffer; /* uint32 */
+    uint32_t meshletCount;
+    uint32_t vertexCount;
+    uint32_t indexCount;
+    uint32_t vertexStride; /* 12 or 32 bytes */
+} mtx_extraction_output;
+
+/* Caller-owned outputs of the asynchronous whole-path call.  counters (device,
+ * uint32[8]) receive {vertexCount, indexCount, meshletCount, activeBlockCount,
+ * status, 0, 0, 0}; they hold the full sizes even when a capacity was short. */
+typedef struct mtx_mesh_buffers {
+    void *vertices;
+    uint64_t vertexCapacity; /* vertices */
+    uint32_t *indices;
+    uint64_t triangleCapacity; /* triangles */
+    mtx_meshlet_descriptor *meshlets; /* optional */
+    uint64_t meshletCapacity;
+    uint32_t *counters;
+    /* Upper bound on active blocks, sizing the scratch of the extraction
+     * (0 = every block of the grid); more active blocks -> MTX_ERR_CAPACITY. */
+    uint64_t maxActiveBlocks;
+} mtx_mesh_buffers;
+
+/* ------------------------------------------------------------ context */
+
+/* Human-readable name of a status code. */
+const char *mtx_status_string(mtx_status s);
+uint32_t mtx_abi_version(void);
+
+/* VulkanContext (src/vulkan_context.h:7-45), compute only: binds a CUDA
+ * device, a stream (NULL = the legacy default stream) and a grow-only
+ * scratch arena. */
+mtx_status mtx_context_create(int device, void *stream, mtx_context_t *out);
+mtx_status mtx_context_destroy(mtx_context_t ctx);
+mtx_status mtx_context_set_stream(mtx_context_t ctx, void *stream);
+/* Last error text of this context ("" if none). */
+const char *mtx_context_last_error(mtx_context_t ctx);
+/* Wait for the stream, then report (and clear) any error a kernel recorded. */
+mtx_status mtx_synchronize(mtx_context_t ctx);
+/* Host-side fault injection for tests: the k-th device allocation from now
+ * fails with MTX_ERR_OOM (k = 0 disables). */
+mtx_status mtx_debug_fail_allocation(mtx_context_t ctx, uint32_t k);
+
+/* ------------------------------------------------------------- volume */
+
+/* loadVolume's in-memory result + the staging upload of computeMinMaxMip
+ * (src/volume.h:14-43, src/minMaxManager.cpp:115-125): copies host voxels
+ * into a new device volume. */
+mtx_status mtx_volume_upload(mtx_context_t ctx, const void *host, const uint32_t dims[3],
+                             uint32_t dtype, mtx_volume *out);
+/* Describes existing device memory as a volume (no copy, not owned). */
+mtx_status mtx_volume_wrap(void *device_ptr, const uint32_t dims[3], uint32_t dtype,
+                           mtx_volume *out);
+mtx_status mtx_volume_free(mtx_context_t ctx, mtx_volume *vol);
+
+/* PushConstants as src/meshtrex.cpp:76-84 fills them, for a cubic block. */
+mtx_status mtx_push_constants_init(const uint32_t dims[3], uint32_t block_edge, float isovalue,
+                                   mtx_push_constants *out);
+/* Decode a min/max key back to the voxel value (u8/u16: the value). */
+float mtx_key_to_float(uint32_t dtype, uint32_t key);
+
+/* ------------------------------------------------------------ stage 1 */
+
+/* computeMinMaxMip (src/minMaxManager.h:20-21, minMaxManager.cpp:63-225):
+ * per-block min/max over (B+1)^3 voxels, then the min/max octree with
+ * 1 + floor(log2(max grid extent)) levels of ceil extents. */
+mtx_status mtx_compute_min_max_mip(mtx_context_t ctx, const mtx_volume *vol,
+                                   const mtx_push_constants *pc, mtx_profiler_t prof,
+                                   mtx_minmax_output *out);
+mtx_status mtx_minmax_free(mtx_context_t ctx, mtx_minmax_output *mm);
+
+/* ------------------------------------------------------------ stage 2 */
+
+/* filterActiveBlocks (src/filteringManager.h:9-10, filteringManager.cpp:20-141):
+ * active = min != max and the isovalue in [min, max] (round(iso) for integer
+ * volumes, blockFilteringTestUtils.h:456-469); compacted in ascending block
+ * order by a single-pass decoupled look-back scan. */
+mtx_status mtx_filter_active_blocks(mtx_context_t ctx, const mtx_minmax_output *mm,
+                                    const mtx_push_constants *pc, mtx_profiler_t prof,
+                                    mtx_filtering_output *out);
+/* readActiveBlockCount (src/filteringManager.h:13, filteringManager.cpp:144-164). */
+mtx_status mtx_read_active_block_count(mtx_context_t ctx, mtx_filtering_output *filt);
+mtx_status mtx_filtering_free(mtx_context_t ctx, mtx_filtering_output *filt);
+
+/* ------------------------------------------------------------ stage 3 */
+
+/* extractMeshletDescriptors (src/extractionManager.h:10-11,
+ * extractionManager.cpp:250-717): PMB marching cubes over the active blocks.
+ * Like meshtrex, returns an empty output when filt->activeBlockCount is 0
+ * (the host count must have been read).  Counts, then allocates the outputs
+ * exactly, then emits; each vertex is written once, by its owning block. */
+mtx_status mtx_extract_meshlet_descriptors(mtx_context_t ctx, const mtx_minmax_output *mm,
+                                           const mtx_filtering_output *filt,
+                                           const mtx_push_constants *pc,
+                                           const mtx_extract_options *opts, mtx_profiler_t prof,
+                                           mtx_extraction_output *out);
+mtx_status mtx_extraction_free(mtx_context_t ctx, mtx_extraction_output *ext);
+
+/* The three stages in one call with caller-owned outputs and no host
+ * synchronisation (main's sequence, src/meshtrex.cpp:107-141, without the
+ * blocking count readback).  Capacity overflow is reported through
+ * counters[4] and mtx_synchronize as MTX_ERR_CAPACITY. */
+mtx_status mtx_extract_plain_async(mtx_context_t ctx, const mtx_volume *vol,
+                                   const mtx_push_constants *pc, const mtx_extract_options *opts,
+                                   const mtx_mesh_buffers *out);
+
+/* ------------------------------------------------------------ profiler */
+
+/* GPUProfiler (src/gpuProfiler.h:11-160): CUDA events around the stage
+ * names MinMax_Leaf_Pass, MinMax_Octree_Reduction, Active_Block_Filtering
+ * and Mesh_Extraction. */
+mtx_status mtx_profiler_create(mtx_context_t ctx, mtx_profiler_t *out);
+mtx_status mtx_profiler_destroy(mtx_profiler_t prof);
+mtx_status mtx_profiler_begin_frame(mtx_profiler_t prof);
+/* Waits for the frame's events and accumulates per-region times. */
+mtx_status mtx_profiler_end_frame(mtx_profiler_t prof);
+uint32_t mtx_profiler_region_count(mtx_profiler_t prof);
+/* name (<= 63 chars + NUL) and the last frame's and running-average time in ms. */
+mtx_status mtx_profiler_region(mtx_profiler_t prof, uint32_t i, char name[64], double *last_ms,
+                               double *avg_ms, uint32_t *frames);
+/* ProfilingManager::exportCSV (src/profilingManager.h:141-171). */
+mtx_status mtx_profiler_export_csv(mtx_profiler_t prof, const char *path);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MESHTREX_MTX_H */

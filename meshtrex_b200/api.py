@@ -1,0 +1,345 @@
+"""Python front end of the C ABI, mirroring meshtrex's stage managers.
+
+  compute_min_max_mip        src/minMaxManager.h:20-21
+  filter_active_blocks       src/filteringManager.h:9-10
+  read_active_block_count    src/filteringManager.h:13
+  extract_meshlet_descriptors src/extractionManager.h:10-11
+
+Torch is used only for device memory and streams: volumes are CUDA tensors
+indexed [z, y, x] and outputs are handed back as views or copies of the
+library's device buffers.  All work runs in libmeshtrex_b200.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+_DT = {torch.uint8: L.DTYPE_U8, torch.uint16: L.DTYPE_U16, torch.float32: L.DTYPE_F32}
+_NP = {np.dtype(np.uint8): L.DTYPE_U8, np.dtype(np.uint16): L.DTYPE_U16,
+       np.dtype(np.float32): L.DTYPE_F32}
+
+
+class _Dev:
+    """Wraps a device pointer so torch can view it without copying."""
+
+    def __init__(self, ptr: int, shape, typestr: str):
+        self.__cuda_array_interface__ = {"shape": tuple(shape), "typestr": typestr,
+                                         "data": (int(ptr or 0), False), "version": 3,
+                                         "strides": None}
+
+
+def device_view(ptr: int, shape, dtype: torch.dtype) -> torch.Tensor:
+    typestr = {torch.uint8: "|u1", torch.uint16: "<u2", torch.uint32: "<u4",
+               torch.float32: "<f4", torch.int32: "<i4"}[dtype]
+    n = int(np.prod(shape))
+    if n == 0 or not ptr:
+        return torch.empty(shape, dtype=dtype, device="cuda")
+    return torch.as_tensor(_Dev(ptr, shape, typestr), device="cuda")
+
+
+def _stream_ptr(stream=None) -> int:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return int(s.cuda_stream)
+
+
+class Context:
+    """VulkanContext's compute role: device, stream, scratch arena."""
+
+    def __init__(self, device: int = 0, stream=None):
+        self.handle = C.c_void_p()
+        L.check(L.lib().mtx_context_create(device, C.c_void_p(_stream_ptr(stream)),
+                                           C.byref(self.handle)), "mtx_context_create")
+
+    def set_stream(self, stream=None):
+        L.check(L.lib().mtx_context_set_stream(self.handle, C.c_void_p(_stream_ptr(stream))),
+                "mtx_context_set_stream", self.handle)
+
+    def synchronize(self):
+        L.check(L.lib().mtx_synchronize(self.handle), "mtx_synchronize", self.handle)
+
+    def fail_allocation(self, k: int):
+        L.check(L.lib().mtx_debug_fail_allocation(self.handle, k), "mtx_debug_fail_allocation")
+
+    def close(self):
+        if self.handle:
+            L.lib().mtx_context_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def push_constants(dims_xyz, block: int, iso: float) -> L.PushConstants:
+    pc = L.PushConstants()
+    d = (C.c_uint32 * 3)(*[int(x) for x in dims_xyz])
+    L.check(L.lib().mtx_push_constants_init(d, int(block), float(iso), C.byref(pc)),
+            "mtx_push_constants_init")
+    return pc
+
+
+def wrap_volume(t: torch.Tensor) -> L.Volume:
+    """Describe a contiguous CUDA tensor [z, y, x] as a volume (no copy)."""
+    assert t.is_cuda and t.is_contiguous() and t.dim() == 3, "volume must be a contiguous CUDA [z,y,x] tensor"
+    v = L.Volume()
+    d = (C.c_uint32 * 3)(t.shape[2], t.shape[1], t.shape[0])
+    L.check(L.lib().mtx_volume_wrap(C.c_void_p(t.data_ptr()), d, _DT[t.dtype], C.byref(v)),
+            "mtx_volume_wrap")
+    return v
+
+
+def upload_volume(ctx: Context, a: np.ndarray) -> L.Volume:
+    """Host array [z, y, x] -> new device volume (meshtrex's staging upload)."""
+    a = np.ascontiguousarray(a)
+    v = L.Volume()
+    d = (C.c_uint32 * 3)(a.shape[2], a.shape[1], a.shape[0])
+    L.check(L.lib().mtx_volume_upload(ctx.handle, C.c_void_p(a.ctypes.data), d, _NP[a.dtype],
+                                      C.byref(v)), "mtx_volume_upload", ctx.handle)
+    return v
+
+
+def free_volume(ctx: Context, v: L.Volume):
+    L.lib().mtx_volume_free(ctx.handle, C.byref(v))
+
+
+@dataclass
+class MinMax:
+    ctx: Context
+    out: L.MinMaxOutput
+
+    @property
+    def levels(self) -> int:
+        return int(self.out.mipLevels)
+
+    def level(self, l: int) -> torch.Tensor:
+        """uint32 [gz, gy, gx, 2] {min,max} keys of mip level l (a copy)."""
+        e = self.out.levelExtent[l]
+        base = self.out.minMaxImage.ptr + 8 * int(self.out.levelOffset[l])
+        return device_view(base, (e[2], e[1], e[0], 2), torch.int32).clone().view(torch.int32)
+
+    def all_levels(self) -> torch.Tensor:
+        n = self.out.minMaxImage.size // 8
+        return device_view(self.out.minMaxImage.ptr, (n, 2), torch.int32).clone()
+
+    def free(self):
+        if self.out.minMaxImage.ptr:
+            L.lib().mtx_minmax_free(self.ctx.handle, C.byref(self.out))
+
+
+@dataclass
+class Filtering:
+    ctx: Context
+    out: L.FilteringOutput
+
+    @property
+    def active_block_count(self) -> int:
+        return int(self.out.activeBlockCount)
+
+    def ids(self) -> torch.Tensor:
+        n = self.out.activeBlockCount
+        return device_view(self.out.compactedBlockIdBuffer.ptr, (n,), torch.int32).clone()
+
+    def device_count(self) -> int:
+        return int(device_view(self.out.activeBlockCountBuffer.ptr, (1,), torch.int32).item())
+
+    def free(self):
+        if self.out.compactedBlockIdBuffer.ptr:
+            L.lib().mtx_filtering_free(self.ctx.handle, C.byref(self.out))
+
+
+@dataclass
+class Extraction:
+    ctx: Context
+    out: L.ExtractionOutput
+
+    @property
+    def vertex_count(self):
+        return int(self.out.vertexCount)
+
+    @property
+    def index_count(self):
+        return int(self.out.indexCount)
+
+    @property
+    def meshlet_count(self):
+        return int(self.out.meshletCount)
+
+    def vertices(self) -> torch.Tensor:
+        """float32 [V, 3] (xyz format) or [V, 8] (VertexData)."""
+        w = self.out.vertexStride // 4
+        return device_view(self.out.vertexBuffer.ptr, (self.out.vertexCount, w), torch.float32).clone()
+
+    def indices(self) -> torch.Tensor:
+        return device_view(self.out.indexBuffer.ptr, (self.out.indexCount // 3, 3), torch.int32).clone()
+
+    def meshlets(self) -> torch.Tensor:
+        return device_view(self.out.meshletDescriptorBuffer.ptr, (self.out.meshletCount, 4),
+                           torch.int32).clone()
+
+    def counters(self) -> torch.Tensor:
+        return device_view(self.out.vertexCountBuffer.ptr, (3,), torch.int32).clone()
+
+    def free(self):
+        if self.out.vertexCountBuffer.ptr or self.out.meshletDescriptorBuffer.ptr:
+            L.lib().mtx_extraction_free(self.ctx.handle, C.byref(self.out))
+
+
+class Profiler:
+    """GPUProfiler analogue: per-stage CUDA-event times under meshtrex's stage names."""
+
+    def __init__(self, ctx: Context):
+        self.ctx = ctx
+        self.handle = C.c_void_p()
+        L.check(L.lib().mtx_profiler_create(ctx.handle, C.byref(self.handle)), "mtx_profiler_create")
+
+    def begin_frame(self):
+        L.lib().mtx_profiler_begin_frame(self.handle)
+
+    def end_frame(self):
+        L.check(L.lib().mtx_profiler_end_frame(self.handle), "mtx_profiler_end_frame")
+
+    def regions(self):
+        out = {}
+        for i in range(L.lib().mtx_profiler_region_count(self.handle)):
+            name = C.create_string_buffer(64)
+            last, avg, fr = C.c_double(), C.c_double(), C.c_uint32()
+            L.lib().mtx_profiler_region(self.handle, i, name, C.byref(last), C.byref(avg), C.byref(fr))
+            out[name.value.decode()] = (last.value, avg.value, fr.value)
+        return out
+
+    def export_csv(self, path: str):
+        L.check(L.lib().mtx_profiler_export_csv(self.handle, path.encode()), "mtx_profiler_export_csv")
+
+    def close(self):
+        if self.handle:
+            L.lib().mtx_profiler_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _prof(p):
+    return p.handle if p is not None else None
+
+
+def compute_min_max_mip(ctx: Context, volume: L.Volume, pc: L.PushConstants, profiler=None) -> MinMax:
+    out = L.MinMaxOutput()
+    L.check(L.lib().mtx_compute_min_max_mip(ctx.handle, C.byref(volume), C.byref(pc), _prof(profiler),
+                                            C.byref(out)), "computeMinMaxMip", ctx.handle)
+    return MinMax(ctx, out)
+
+
+def filter_active_blocks(ctx: Context, mm: MinMax, pc: L.PushConstants, profiler=None) -> Filtering:
+    out = L.FilteringOutput()
+    L.check(L.lib().mtx_filter_active_blocks(ctx.handle, C.byref(mm.out), C.byref(pc),
+                                             _prof(profiler), C.byref(out)),
+            "filterActiveBlocks", ctx.handle)
+    return Filtering(ctx, out)
+
+
+def read_active_block_count(ctx: Context, f: Filtering) -> int:
+    L.check(L.lib().mtx_read_active_block_count(ctx.handle, C.byref(f.out)), "readActiveBlockCount",
+            ctx.handle)
+    return f.active_block_count
+
+
+def extract_options(vertex_format=L.VERTEX_XYZ, frame=L.FRAME_VOXEL, normals=False,
+                    staging=L.STAGING_AUTO, threads=0, cell_cases: torch.Tensor | None = None):
+    o = L.ExtractOptions()
+    o.vertexFormat, o.frame, o.normals = vertex_format, frame, int(bool(normals))
+    o.staging, o.threads = staging, threads
+    o.cellCases = cell_cases.data_ptr() if cell_cases is not None else None
+    return o
+
+
+def extract_meshlet_descriptors(ctx: Context, mm: MinMax, f: Filtering, pc: L.PushConstants,
+                                options: L.ExtractOptions | None = None, profiler=None) -> Extraction:
+    out = L.ExtractionOutput()
+    opts = options if options is not None else extract_options()
+    L.check(L.lib().mtx_extract_meshlet_descriptors(ctx.handle, C.byref(mm.out), C.byref(f.out),
+                                                    C.byref(pc), C.byref(opts), _prof(profiler),
+                                                    C.byref(out)),
+            "extractMeshletDescriptors", ctx.handle)
+    return Extraction(ctx, out)
+
+
+@dataclass
+class Mesh:
+    vertices: torch.Tensor   # float32 [V, 3] or [V, 8]
+    indices: torch.Tensor    # int32 [T, 3] (uint32 bit pattern)
+    meshlets: torch.Tensor   # int32 [M, 4]
+    active_ids: torch.Tensor
+    leaf: torch.Tensor
+
+
+def extract(volume: torch.Tensor, block: int, iso: float, ctx: Context | None = None,
+            options: L.ExtractOptions | None = None, profiler=None) -> Mesh:
+    """The plain drop-in path, stage by stage, on a CUDA volume tensor [z, y, x]."""
+    own = ctx is None
+    ctx = ctx or Context()
+    v = wrap_volume(volume)
+    pc = push_constants((volume.shape[2], volume.shape[1], volume.shape[0]), block, iso)
+    mm = compute_min_max_mip(ctx, v, pc, profiler)
+    f = filter_active_blocks(ctx, mm, pc, profiler)
+    read_active_block_count(ctx, f)
+    x = extract_meshlet_descriptors(ctx, mm, f, pc, options, profiler)
+    ctx.synchronize()
+    m = Mesh(x.vertices(), x.indices(), x.meshlets(), f.ids(), mm.level(0))
+    x.free()
+    f.free()
+    mm.free()
+    if own:
+        ctx.close()
+    return m
+
+
+class AsyncExtractor:
+    """The whole plain path with preallocated outputs and no host sync
+    (mtx_extract_plain_async); capturable in a CUDA graph once warmed up."""
+
+    def __init__(self, ctx: Context, volume: torch.Tensor, block: int, iso: float,
+                 vertex_capacity: int, triangle_capacity: int, max_active_blocks: int = 0,
+                 options: L.ExtractOptions | None = None):
+        self.ctx = ctx
+        self.volume = volume
+        self.vol = wrap_volume(volume)
+        self.pc = push_constants((volume.shape[2], volume.shape[1], volume.shape[0]), block, iso)
+        self.opts = options if options is not None else extract_options()
+        w = 3 if self.opts.vertexFormat == L.VERTEX_XYZ else 8
+        self.vertices = torch.empty((vertex_capacity, w), dtype=torch.float32, device="cuda")
+        self.indices = torch.empty((triangle_capacity, 3), dtype=torch.int32, device="cuda")
+        self.counters = torch.zeros(8, dtype=torch.int32, device="cuda")
+        self.bufs = L.MeshBuffers()
+        self.bufs.vertices = self.vertices.data_ptr()
+        self.bufs.vertexCapacity = vertex_capacity
+        self.bufs.indices = self.indices.data_ptr()
+        self.bufs.triangleCapacity = triangle_capacity
+        self.bufs.meshlets = None
+        self.bufs.meshletCapacity = 0
+        self.bufs.counters = self.counters.data_ptr()
+        self.bufs.maxActiveBlocks = max_active_blocks
+
+    def set_iso(self, iso: float):
+        self.pc.isovalue = float(iso)
+
+    def run(self):
+        L.check(L.lib().mtx_extract_plain_async(self.ctx.handle, C.byref(self.vol), C.byref(self.pc),
+                                                C.byref(self.opts), C.byref(self.bufs)),
+                "mtx_extract_plain_async", self.ctx.handle)

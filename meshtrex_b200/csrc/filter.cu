@@ -1,0 +1,136 @@
+// Stage 2: active-block filtering with ordered stream compaction
+// (meshtrex: occupiedBlockPrefixSum.comp.glsl:50-177, dispatched by
+// activeBlockFilteringPass.cpp:87-153; CPU rule blockFilteringTestUtils.h:438-478).
+//
+// meshtrex scans within a workgroup and then takes one atomicAdd per
+// workgroup, so the compacted list is ordered only inside a workgroup.  Here
+// each CTA takes a tile of 1024 consecutive block ids by ticket, counts its
+// active blocks (warp scan + CTA scan), and resolves its global offset with a
+// single-pass decoupled look-back over the tiles before it: the list comes out
+// in ascending block order, which is the order the CPU rule produces.
+#include "mtx_internal.h"
+
+namespace mtx {
+
+constexpr int kFilterThreads = 256;
+constexpr int kFilterItems = 4;
+constexpr int kFilterTile = kFilterThreads * kFilterItems;
+
+// tile status word: [31:30] flag (0 empty, 1 aggregate, 2 inclusive, 3 aborted), [29:0] count
+constexpr uint32_t kFlagAgg = 1u, kFlagInc = 2u, kFlagAbort = 3u;
+
+__global__ void __launch_bounds__(kFilterThreads)
+    filter_compact_kernel(const uint2 *__restrict__ leaf, uint64_t nblocks, uint32_t ntiles, uint32_t dtype,
+                          float iso, uint32_t *__restrict__ ids, uint32_t *__restrict__ rank_map,
+                          uint32_t *__restrict__ count_out, uint64_t *__restrict__ count_status,
+                          uint32_t *tile_status, uint32_t *ticket, DevStatus *st) {
+    __shared__ uint32_t s_tile, s_prefix, s_abort;
+    __shared__ uint32_t s_tmp[kFilterThreads / 32 + 1];
+    if (threadIdx.x == 0) {
+        s_tile = atomicAdd(ticket, 1u);
+        s_abort = 0;
+    }
+    __syncthreads();
+    const uint32_t t = s_tile;
+    if (t >= ntiles) return;
+
+    const uint64_t base = (uint64_t)t * kFilterTile + (uint64_t)threadIdx.x * kFilterItems;
+    uint32_t f[kFilterItems];
+    if (base + kFilterItems <= nblocks) {
+        const uint4 *p = reinterpret_cast<const uint4 *>(leaf + base);
+        uint4 a = __ldg(p), b = __ldg(p + 1);
+        f[0] = block_active(dtype, a.x, a.y, iso);
+        f[1] = block_active(dtype, a.z, a.w, iso);
+        f[2] = block_active(dtype, b.x, b.y, iso);
+        f[3] = block_active(dtype, b.z, b.w, iso);
+    } else {
+#pragma unroll
+        for (int i = 0; i < kFilterItems; ++i) {
+            f[i] = 0;
+            if (base + i < nblocks) {
+                uint2 v = leaf[base + i];
+                f[i] = block_active(dtype, v.x, v.y, iso);
+            }
+        }
+    }
+    const uint32_t c = f[0] + f[1] + f[2] + f[3];
+    uint32_t total;
+    const uint32_t excl = cta_exclusive_scan<kFilterThreads>(c, s_tmp, &total);
+
+    if (threadIdx.x < 32) {
+        const uint32_t lane = threadIdx.x;
+        uint32_t prefix = 0;
+        bool abort = false;
+        if (t == 0) {
+            if (lane == 0) st_volatile(&tile_status[0], (kFlagInc << 30) | total);
+        } else {
+            if (lane == 0) st_volatile(&tile_status[t], (kFlagAgg << 30) | total);
+            int64_t j = (int64_t)t - 1;
+            uint32_t spins = 0;
+            while (true) {
+                const int64_t k = j - (int64_t)lane;
+                const uint32_t w = k >= 0 ? ld_volatile(&tile_status[k]) : (kFlagInc << 30);
+                const uint32_t flag = w >> 30;
+                if (__any_sync(0xffffffffu, flag == kFlagAbort)) { abort = true; break; }
+                const uint32_t inc = __ballot_sync(0xffffffffu, flag == kFlagInc);
+                const uint32_t emp = __ballot_sync(0xffffffffu, flag == 0u);
+                const uint32_t first = inc ? (uint32_t)(__ffs(inc) - 1) : 32u;
+                const uint32_t window = first >= 31 ? 0xffffffffu : ((2u << first) - 1u);
+                if (emp & window) {
+                    if (++spins >= kSpinLimit) {
+                        if (lane == 0) report(st, MTX_ERR_TIMEOUT, kSiteFilterLookback, t, (uint32_t)j);
+                        abort = true;
+                        break;
+                    }
+                    backoff(spins);
+                    continue;
+                }
+                uint32_t v = lane <= first ? (w & 0x3fffffffu) : 0u;
+#pragma unroll
+                for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+                prefix += v;
+                if (first < 32) break;
+                j -= 32;
+            }
+            if (lane == 0)
+                st_volatile(&tile_status[t], abort ? (kFlagAbort << 30) : ((kFlagInc << 30) | (prefix + total)));
+        }
+        if (lane == 0) {
+            s_prefix = prefix;
+            s_abort = abort ? 1u : 0u;
+        }
+    }
+    __syncthreads();
+    if (s_abort) return;
+    uint32_t r = s_prefix + excl;
+#pragma unroll
+    for (int i = 0; i < kFilterItems; ++i) {
+        if (f[i]) {
+            const uint32_t id = (uint32_t)(base + i);
+            ids[r] = id;
+            rank_map[id] = r;
+            if (count_status) count_status[r] = 0ull;
+            ++r;
+        }
+    }
+    if (t == ntiles - 1 && threadIdx.x == 0) *count_out = s_prefix + total;
+}
+
+mtx_status launch_filter(mtx_context *c, const Problem &p, const uint2 *leaf, uint32_t *ids, uint32_t *rank_map,
+                         uint32_t *count, uint64_t *count_status, cudaStream_t s) {
+    if (p.nblocks >= (1ull << 30)) return fail(c, MTX_ERR_UNSUPPORTED, "more than 2^30 blocks");
+    const uint32_t ntiles = (uint32_t)((p.nblocks + kFilterTile - 1) / kFilterTile);
+    mtx_status rs = scratch_reserve(c, c->filter_status, sizeof(uint32_t) * (size_t)ntiles);
+    if (rs != MTX_OK) return rs;
+    MTX_CUDA(c, cudaMemsetAsync(c->filter_status.ptr, 0, sizeof(uint32_t) * (size_t)ntiles, s));
+    MTX_CUDA(c, cudaMemsetAsync(&c->ctrl->filter_ticket, 0, sizeof(uint32_t), s));
+    MTX_CUDA(c, cudaMemsetAsync(count, 0, sizeof(uint32_t), s));
+    filter_compact_kernel<<<ntiles, kFilterThreads, 0, s>>>(
+        leaf, p.nblocks, ntiles, p.dtype, p.iso, ids, rank_map, count, count_status,
+        (uint32_t *)c->filter_status.ptr, &c->ctrl->filter_ticket, &c->ctrl->status);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(c, e, "filter launch");
+    return MTX_OK;
+}
+
+}  // namespace mtx
