@@ -1,0 +1,441 @@
+#!/usr/bin/env python
+"""Benchmark of the isosurface-extraction path on B200.
+
+Workload (one step): the 1024^3 uint16 fBm ball (block 8^3) extracted at
+isovalues 16384, 32768 and 49152 as three separate plain extractions, each
+min/max + octree -> filter + compaction -> PMB count -> PMB emit, with the
+volume already resident in HBM (2 GiB, larger than L2, so every extraction
+streams it from DRAM).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mtx|reference]
+
+With N > 1 it is launched by torchrun, one rank per GPU; every rank extracts
+its own copy of the workload (independent replicas, weak scaling) and the
+step time is the maximum over ranks.  `--impl reference` times the CPU
+restatement of meshtrex's path (the oracle, all host threads) on a bounded
+z-slab sample of the same workload.
+
+Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+import torch  # noqa: E402
+
+METRIC = "Gvoxels/s + tris/s vs HBM roofline: plain vs batched; bwd/fwd time ratio"
+N = 1024  # volume edge; --size changes it for profiling runs only
+BLOCK = 8
+ISOS = (16384.0, 32768.0, 49152.0)
+def workload():
+    return (f"plain {N}^3 uint16 fBm ball, block 8^3, isovalues 16384/32768/49152 as three "
+            "separate plain extractions per step")
+FALLBACK_HBM_GBS = 6650.0
+
+
+# ------------------------------------------------------------------ infra
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons over a window."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons, n = [], None, set(), 0
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax = float(parts[2])
+                except ValueError:
+                    continue
+                n += 1
+                for name, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(name)
+        os.remove(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": n}
+
+
+def nproc():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+# --------------------------------------------------------------- CPU side
+def cpu_sample_volume(nz: int, device: str):
+    """Middle z-slab of nz slices of the 1024^3 workload, as a host array."""
+    from meshtrex_b200 import synth
+    z0 = (N - nz) // 2
+    t = synth.fbm_ball(N, seed=1, device=device, zslab=(z0, z0 + nz))
+    return t.cpu().view(torch.int16).numpy().view(np.uint16), z0
+
+
+def time_cpu_oracle(vol: np.ndarray, threads: int):
+    """One step of the CPU restatement on `vol`: the three isovalues."""
+    from oracle import oracle as O
+    t0 = time.perf_counter()
+    tris = 0
+    for iso in ISOS:
+        _, _, t = O.pipeline(vol, BLOCK, iso, nthreads=threads)
+        tris += t
+    return time.perf_counter() - t0, tris
+
+
+def cpu_baseline(vol: np.ndarray, threads: int, target_s: float = 10.0):
+    """The oracle timed on the host cores on the same volume, repeated to ~target_s."""
+    secs, tris, reps = 0.0, 0, 0
+    while reps == 0 or (secs < target_s and reps < 20):
+        s, t = time_cpu_oracle(vol, threads)
+        secs += s
+        tris += t
+        reps += 1
+    vox = 3 * vol.size * reps
+    return {"value": vox / secs / 1e9, "unit": "Gvoxels/s", "cores": threads, "kind": "port",
+            "sample": (f"the whole {vol.shape[2]}x{vol.shape[1]}x{vol.shape[0]} uint16 volume at the three "
+                       f"isovalues, {reps} repetition(s), {secs:.2f} s"),
+            "tris_per_s": tris / secs}
+
+
+def run_reference(args):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    threads = nproc()
+    # calibrate the sample so that one step is ~10 s of CPU work
+    probe, _ = cpu_sample_volume(min(N, 64), dev)
+    secs, _ = time_cpu_oracle(probe, threads)
+    pz = probe.shape[0]
+    total_steps = args.steps + args.warmup
+    budget = 150.0  # seconds for the whole run
+    nz = int(min(N, pz * 10.0 / max(secs, 1e-3), pz * budget / max(secs * total_steps, 1e-3)))
+    nz = max(16, (nz // 8) * 8)
+    vol, z0 = cpu_sample_volume(nz, dev)
+    for _ in range(args.warmup):
+        time_cpu_oracle(vol, threads)
+    t_all, tris_all = 0.0, 0
+    for _ in range(args.steps):
+        s, t = time_cpu_oracle(vol, threads)
+        t_all += s
+        tris_all += t
+    vox = 3 * vol.size * args.steps
+    value = vox / t_all / 1e9
+    line = {"metric": METRIC, "impl": "reference", "value": value, "unit": "Gvoxels/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * t_all / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16",
+            "data": "synthetic (seeded fBm ball, same generator as the GPU arm)",
+            "config": {"workload": workload(), "sample": f"1024x1024x{nz} middle z-slab per step",
+                       "block": BLOCK, "isovalues": list(ISOS), "parallelism": "CPU, all host threads"},
+            "tris_per_s": tris_all / t_all,
+            "cpu_baseline": {"value": value, "unit": "Gvoxels/s", "cores": threads, "kind": "port",
+                             "sample": f"1024x1024x{nz} middle z-slab (z={z0}..{z0 + nz}), 3 isovalues"},
+            "e2e": {"value": value, "unit": "Gvoxels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------- GPU side
+def launches_per_extraction(grid):
+    m = max(grid)
+    levels = 1
+    while m > 1:
+        m >>= 1
+        levels += 1
+    return 1 + (levels + 1) // 3 + 1 + 1 + 1  # leaf, octree launches, filter, count, emit
+
+
+def read_traffic():
+    """DRAM bytes per 1024^3 min/max launch from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "minmax_leaf_u16_b8.txt")
+    try:
+        for line in open(p):
+            if line.startswith("dram_bytes_per_launch_1024^3:"):
+                return float(line.split(":")[1])
+    except Exception:
+        pass
+    return None
+
+
+def run_mtx(args):
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    from meshtrex_b200 import api, synth
+
+    vol = load_or_make_volume(args.cache)
+    torch.cuda.synchronize()
+    ctx = api.Context(local)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream)
+
+    # size the outputs from one drop-in extraction per isovalue
+    caps = []
+    for iso in ISOS:
+        m = api.extract(vol, BLOCK, iso, ctx=ctx)
+        caps.append((m.vertices.shape[0], m.indices.shape[0], m.active_ids.shape[0]))
+        del m
+    exts = [api.AsyncExtractor(ctx, vol, BLOCK, iso, v + 1024, t + 1024, max_active_blocks=a + 1024)
+            for iso, (v, t, a) in zip(ISOS, caps)]
+
+    def step():
+        for e in exts:
+            e.run()
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    ctx.synchronize()
+
+    prof = api.Profiler(ctx)
+    clocks = Clocks(local)
+    clocks.start()
+    # keep the GPU busy for >= 1 s before the timed steps so the clock samples see load
+    t_soak = time.perf_counter()
+    while time.perf_counter() - t_soak < 1.0:
+        step()
+        torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    ctx.set_profiler(prof)
+    prof.begin_frame()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    prof.end_frame()
+    ctx.set_profiler(None)
+    ctx.synchronize()  # raises on any device-side error
+    ms = e0.elapsed_time(e1)
+    t_local = ms / 1000.0
+    if ws > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([t_local], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+    else:
+        t_max = t_local
+    counters = [e.counters.cpu().numpy().view(np.uint32) for e in exts]
+    for c in counters:
+        assert c[4] == 0, f"device status {c[4]}"
+    V = [int(c[0]) for c in counters]
+    T = [int(c[1]) // 3 for c in counters]
+    nvox = N ** 3
+    steps = args.steps
+    value = ws * 3 * nvox * steps / t_max / 1e9
+    tris_s = ws * sum(T) * steps / t_max
+
+    regions = prof.regions()
+    prof.close()
+    # one profiler frame covers the K timed steps: per-extraction stage times
+    per_stage = {k: regions[k][0] / (3 * steps) for k in regions}
+    peak, peak_kind = peak_hbm()
+    leaf_ms = per_stage.get("MinMax_Leaf_Pass")
+    grid = ((N + BLOCK - 1) // BLOCK,) * 3
+    nblocks = grid[0] * grid[1] * grid[2]
+    leaf_bytes = nvox * 2 + nblocks * 8
+    achieved = leaf_bytes / (leaf_ms / 1000.0) / 1e9 if leaf_ms else None
+    traffic = read_traffic()
+    step_bytes = 3 * nvox * 2 + sum(v * 12 + t * 12 for v, t in zip(V, T))
+    pipe_gbs = step_bytes * steps / t_local / 1e9
+
+    line = {"metric": METRIC, "value": value, "unit": "Gvoxels/s", "n_gpus": ws, "steps": steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * t_max / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u16",
+            "data": "synthetic (seeded fBm ball generated on the device; no dataset)",
+            "config": {"workload": workload(), "volume": [N, N, N], "block": BLOCK, "isovalues": list(ISOS),
+                       "l2": "inputs larger than L2 (2 GiB volume streamed per extraction)",
+                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
+            "tris_per_s": tris_s, "vertices_per_step": sum(V), "triangles_per_step": sum(T),
+            "stages_ms_per_extraction": per_stage,
+            "roofline": {"bound": "hbm", "kernel": "minmax_leaf_vec_kernel<uint16_t,8>",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": (achieved / peak) if achieved else None,
+                         "traffic": traffic, "algorithmic_bytes": leaf_bytes, "peak_kind": f"{peak_kind} (burst copy)"},
+            "pipeline_roofline": {"achieved": pipe_gbs, "peak": peak, "unit": "GB/s", "frac": pipe_gbs / peak,
+                                  "bytes_per_step": step_bytes,
+                                  "what": "volume read once per extraction + mesh written (12 B/vertex, 12 B/triangle)"},
+            "gpu_launches": launches_per_extraction(grid) * 3 * steps,
+            "clocks": clk}
+
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        host = vol.cpu().view(torch.int16).numpy().view(np.uint16)
+        line["cpu_baseline"] = cpu_baseline(host, nproc())
+        del host
+
+    if not args.no_e2e:
+        line["e2e"] = run_e2e(ctx, vol, ws, steps=max(1, min(3, steps)))
+
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def load_or_make_volume(cache):
+    """The fBm ball on the device; with --cache, read from / saved to a raw file."""
+    from meshtrex_b200 import synth
+    if cache and os.path.exists(cache) and os.path.getsize(cache) == 2 * N ** 3:
+        a = np.fromfile(cache, dtype=np.int16).reshape(N, N, N)
+        return torch.from_numpy(a).cuda().view(torch.uint16)
+    vol = synth.fbm_ball(N, seed=1, device="cuda")
+    if cache:
+        vol.cpu().view(torch.int16).numpy().tofile(cache)
+    return vol
+
+
+def run_e2e(ctx, vol_dev, ws, steps):
+    """The drop-in C-ABI path from pinned host memory: per extraction, upload
+    (mtx_volume_upload), computeMinMaxMip, filterActiveBlocks,
+    readActiveBlockCount, extractMeshletDescriptors, and the mesh read back
+    to pinned host buffers."""
+    import ctypes as C
+
+    from meshtrex_b200 import _lib as L
+    from meshtrex_b200 import api
+    host = torch.empty(vol_dev.shape, dtype=vol_dev.dtype, pin_memory=True)
+    host.copy_(vol_dev)
+    dims = (C.c_uint32 * 3)(N, N, N)
+    out_v = torch.empty(1, dtype=torch.float32, pin_memory=True)
+    out_i = torch.empty(1, dtype=torch.int32, pin_memory=True)
+    h2d = d2h = 0
+    torch.cuda.synchronize()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for iso in ISOS:
+            v = L.Volume()
+            L.check(L.lib().mtx_volume_upload(ctx.handle, C.c_void_p(host.data_ptr()), dims, L.DTYPE_U16,
+                                              C.byref(v)), "upload", ctx.handle)
+            pc = api.push_constants((N, N, N), BLOCK, iso)
+            mm = api.compute_min_max_mip(ctx, v, pc)
+            f = api.filter_active_blocks(ctx, mm, pc)
+            api.read_active_block_count(ctx, f)
+            x = api.extract_meshlet_descriptors(ctx, mm, f, pc)
+            nv, ni = x.out.vertexBuffer.size, x.out.indexBuffer.size
+            if out_v.numel() * 4 < nv:
+                out_v = torch.empty(nv // 4 + 1, dtype=torch.float32, pin_memory=True)
+            if out_i.numel() * 4 < ni:
+                out_i = torch.empty(ni // 4 + 1, dtype=torch.int32, pin_memory=True)
+            # device -> pinned host copies of the mesh
+            if nv:
+                out_v[: nv // 4].copy_(api.device_view(x.out.vertexBuffer.ptr, (nv // 4,), torch.float32))
+            if ni:
+                out_i[: ni // 4].copy_(api.device_view(x.out.indexBuffer.ptr, (ni // 4,), torch.int32))
+            torch.cuda.synchronize()
+            h2d += v.data.size
+            d2h += nv + ni
+            x.free()
+            f.free()
+            mm.free()
+            L.lib().mtx_volume_free(ctx.handle, C.byref(v))
+    torch.cuda.synchronize()
+    t = time.perf_counter() - t0
+    if ws > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([t], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t = float(tt.item())
+    return {"value": ws * 3 * N ** 3 * steps / t / 1e9, "unit": "Gvoxels/s",
+            "h2d_bytes_per_step": h2d // steps, "d2h_bytes_per_step": d2h // steps, "steps": steps,
+            "what": "mtx_volume_upload from pinned host memory -> computeMinMaxMip -> filterActiveBlocks -> "
+                    "readActiveBlockCount -> extractMeshletDescriptors -> mesh copied to pinned host memory"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="mtx", choices=["mtx", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    ap.add_argument("--size", type=int, default=1024, help="volume edge (profiling runs only)")
+    ap.add_argument("--cache", default="", help="raw file to read/write the generated volume")
+    args = ap.parse_args()
+    global N
+    N = args.size
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_mtx(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

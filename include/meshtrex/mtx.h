@@ -274,6 +274,11 @@ uint32_t mtx_profiler_region_count(mtx_profiler_t prof);
 /* name (<= 63 chars + NUL) and the last frame's and running-average time in ms. */
 mtx_status mtx_profiler_region(mtx_profiler_t prof, uint32_t i, char name[64], double *last_ms,
                                double *avg_ms, uint32_t *frames);
+/* Records the stage times of every later call on this context that is not
+ * given its own profiler, the asynchronous whole-path call included (NULL
+ * turns it off); the GPUProfiler* argument of meshtrex's managers made
+ * context-wide (src/minMaxManager.h:21). */
+mtx_status mtx_context_set_profiler(mtx_context_t ctx, mtx_profiler_t prof);
 /* ProfilingManager::exportCSV (src/profilingManager.h:141-171). */
 mtx_status mtx_profiler_export_csv(mtx_profiler_t prof, const char *path);
 

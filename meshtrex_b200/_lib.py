@@ -116,6 +116,7 @@ SIGNATURES = [
     ("mtx_extract_plain_async", _ST, [_P, C.POINTER(Volume), C.POINTER(PushConstants),
                                       C.POINTER(ExtractOptions), C.POINTER(MeshBuffers)]),
     ("mtx_profiler_create", _ST, [_P, C.POINTER(_P)]),
+    ("mtx_context_set_profiler", _ST, [_P, _P]),
     ("mtx_profiler_destroy", _ST, [_P]),
     ("mtx_profiler_begin_frame", _ST, [_P]),
     ("mtx_profiler_end_frame", _ST, [_P]),

@@ -62,6 +62,10 @@ class Context:
     def synchronize(self):
         L.check(L.lib().mtx_synchronize(self.handle), "mtx_synchronize", self.handle)
 
+    def set_profiler(self, prof):
+        L.check(L.lib().mtx_context_set_profiler(self.handle, prof.handle if prof else None),
+                "mtx_context_set_profiler")
+
     def fail_allocation(self, k: int):
         L.check(L.lib().mtx_debug_fail_allocation(self.handle, k), "mtx_debug_fail_allocation")
 

@@ -381,6 +381,7 @@ float mtx_key_to_float(uint32_t dtype, uint32_t key) { return key_to_float(dtype
 mtx_status mtx_compute_min_max_mip(mtx_context_t c, const mtx_volume *vol, const mtx_push_constants *pc,
                                    mtx_profiler_t prof, mtx_minmax_output *out) {
     if (!c || !out) return MTX_ERR_INVALID_ARG;
+    if (!prof) prof = c->prof;
     mtx_status r = check_volume(c, vol);
     if (r != MTX_OK) return r;
     if ((r = check_pc(c, vol, pc)) != MTX_OK) return r;
@@ -432,6 +433,7 @@ mtx_status mtx_minmax_free(mtx_context_t c, mtx_minmax_output *mm) {
 mtx_status mtx_filter_active_blocks(mtx_context_t c, const mtx_minmax_output *mm, const mtx_push_constants *pc,
                                     mtx_profiler_t prof, mtx_filtering_output *out) {
     if (!c || !mm || !out || !mm->minMaxImage.ptr) return c ? fail(c, MTX_ERR_INVALID_ARG, "null argument") : MTX_ERR_INVALID_ARG;
+    if (!prof) prof = c->prof;
     mtx_status r = check_pc(c, &mm->volumeImage, pc);
     if (r != MTX_OK) return r;
     DeviceGuard g(c->device);
@@ -498,6 +500,7 @@ mtx_status mtx_extract_meshlet_descriptors(mtx_context_t c, const mtx_minmax_out
                                            const mtx_extract_options *opts_in, mtx_profiler_t prof,
                                            mtx_extraction_output *out) {
     if (!c || !mm || !f || !out) return c ? fail(c, MTX_ERR_INVALID_ARG, "null argument") : MTX_ERR_INVALID_ARG;
+    if (!prof) prof = c->prof;
     mtx_status r = check_pc(c, &mm->volumeImage, pc);
     if (r != MTX_OK) return r;
     DeviceGuard g(c->device);
@@ -538,6 +541,7 @@ mtx_status mtx_extract_meshlet_descriptors(mtx_context_t c, const mtx_minmax_out
     a.host_count = n;
     a.desc = (mtx_meshlet_descriptor *)desc;
     a.desc_capacity = n;
+    a.block_capacity = n;
     a.faces = (uint32_t *)c->faces.ptr;
     a.count_status = (uint64_t *)c->count_status.ptr;
     a.totals = (uint32_t *)counters;
@@ -612,7 +616,13 @@ mtx_status mtx_extract_plain_async(mtx_context_t c, const mtx_volume *vol, const
     const Problem p = make_problem(vol, pc->blockDim[0], pc->isovalue);
     const uint64_t maxa = out->maxActiveBlocks ? std::min<uint64_t>(out->maxActiveBlocks, p.nblocks) : p.nblocks;
     const uint32_t B = p.B;
-    if ((r = scratch_reserve(c, c->leaf, p.nblocks * 8)) != MTX_OK) return r;
+    const uint32_t grid[3] = {p.GX, p.GY, p.GZ};
+    const int L = mip_levels(grid);
+    if (L > MTX_MAX_MIP_LEVELS) return fail(c, MTX_ERR_UNSUPPORTED, "too many mip levels");
+    uint32_t ext[MTX_MAX_MIP_LEVELS][3];
+    uint64_t off[MTX_MAX_MIP_LEVELS], texels = 0;
+    mip_layout(grid, L, ext, off, &texels);
+    if ((r = scratch_reserve(c, c->leaf, texels * 8)) != MTX_OK) return r;
     if ((r = scratch_reserve(c, c->ids, p.nblocks * 4)) != MTX_OK) return r;
     if ((r = scratch_reserve(c, c->rank, p.nblocks * 4)) != MTX_OK) return r;
     if ((r = scratch_reserve(c, c->count_status, p.nblocks * 8)) != MTX_OK) return r;
@@ -625,10 +635,22 @@ mtx_status mtx_extract_plain_async(mtx_context_t c, const mtx_volume *vol, const
         dcap = maxa;
     }
     cudaStream_t s = c->stream;
-    if ((r = launch_minmax_leaf(c, p, (uint2 *)c->leaf.ptr, s)) != MTX_OK) return r;
-    if ((r = launch_filter(c, p, (const uint2 *)c->leaf.ptr, (uint32_t *)c->ids.ptr, (uint32_t *)c->rank.ptr,
-                           &c->ctrl->active_count, (uint64_t *)c->count_status.ptr, s)) != MTX_OK)
-        return r;
+    mtx_profiler *P = c->prof;
+    prof_begin(P, "MinMax_Leaf_Pass", s);
+    r = launch_minmax_leaf(c, p, (uint2 *)c->leaf.ptr, s);
+    prof_end(P, s);
+    if (r != MTX_OK) return r;
+    if (L > 1) {
+        prof_begin(P, "MinMax_Octree_Reduction", s);
+        r = launch_pyramid(c, (uint2 *)c->leaf.ptr, L, ext, off, s);
+        prof_end(P, s);
+        if (r != MTX_OK) return r;
+    }
+    prof_begin(P, "Active_Block_Filtering", s);
+    r = launch_filter(c, p, (const uint2 *)c->leaf.ptr, (uint32_t *)c->ids.ptr, (uint32_t *)c->rank.ptr,
+                      &c->ctrl->active_count, (uint64_t *)c->count_status.ptr, s);
+    prof_end(P, s);
+    if (r != MTX_OK) return r;
     ExtractArgs a;
     memset(&a, 0, sizeof(a));
     a.ids = (const uint32_t *)c->ids.ptr;
@@ -637,6 +659,7 @@ mtx_status mtx_extract_plain_async(mtx_context_t c, const mtx_volume *vol, const
     a.host_count = 0;
     a.desc = desc;
     a.desc_capacity = dcap;
+    a.block_capacity = maxa;
     a.faces = (uint32_t *)c->faces.ptr;
     a.count_status = (uint64_t *)c->count_status.ptr;
     a.totals = out->counters;
@@ -650,8 +673,14 @@ mtx_status mtx_extract_plain_async(mtx_context_t c, const mtx_volume *vol, const
     a.normals = o.normals;
     a.staging = o.staging;
     a.threads = o.threads;
-    if ((r = launch_count(c, p, a, s)) != MTX_OK) return r;
-    if ((r = launch_emit(c, p, a, s)) != MTX_OK) return r;
+    prof_begin(P, "Mesh_Extraction_Count", s);
+    r = launch_count(c, p, a, s);
+    prof_end(P, s);
+    if (r != MTX_OK) return r;
+    prof_begin(P, "Mesh_Extraction_Emit", s);
+    r = launch_emit(c, p, a, s);
+    prof_end(P, s);
+    if (r != MTX_OK) return r;
     if (desc != out->meshlets && out->meshlets && out->meshletCapacity) {
         // the caller's descriptor buffer was too small for the bound: copy what fits
         MTX_CUDA(c, cudaMemcpyAsync(out->meshlets, desc, out->meshletCapacity * sizeof(mtx_meshlet_descriptor),
@@ -671,8 +700,15 @@ mtx_status mtx_profiler_create(mtx_context_t c, mtx_profiler_t *out) {
     return MTX_OK;
 }
 
+mtx_status mtx_context_set_profiler(mtx_context_t c, mtx_profiler_t p) {
+    if (!c) return MTX_ERR_INVALID_ARG;
+    c->prof = p;
+    return MTX_OK;
+}
+
 mtx_status mtx_profiler_destroy(mtx_profiler_t p) {
     if (!p) return MTX_ERR_INVALID_ARG;
+    if (p->ctx && p->ctx->prof == p) p->ctx->prof = nullptr;
     DeviceGuard g(p->ctx->device);
     for (auto &q : p->pending) {
         cudaEventDestroy(q.a);

@@ -197,7 +197,8 @@ __global__ void __launch_bounds__(NT) count_kernel(Problem p, const __grid_const
                                                    mtx_meshlet_descriptor *__restrict__ desc,
                                                    uint64_t desc_capacity, uint32_t *__restrict__ faces,
                                                    uint64_t *status, uint32_t *ticket, uint32_t *totals,
-                                                   uint8_t *__restrict__ cell_cases, DevStatus *st) {
+                                                   uint8_t *__restrict__ cell_cases, uint64_t block_cap,
+                                                   DevStatus *st) {
     extern __shared__ __align__(128) unsigned char smem[];
     const Plan pl = make_plan(p.B, sizeof(T), tma, false);
     uint32_t *rows = reinterpret_cast<uint32_t *>(smem + pl.off_rows);
@@ -220,6 +221,14 @@ __global__ void __launch_bounds__(NT) count_kernel(Problem p, const __grid_const
     const uint32_t count = *count_ptr;
     const uint32_t B = p.B, BB = B * B;
     uint32_t phase = 0;
+    if (count > block_cap || count > desc_capacity) {
+        // scratch sized for fewer active blocks: report the needed count, do nothing
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            report(st, MTX_ERR_CAPACITY, kSiteEmitCapacity, count, 3);
+            totals[3] = count;
+        }
+        return;
+    }
 
     while (true) {
         if (threadIdx.x == 0) misc[32] = atomicAdd(ticket, 1u);
@@ -445,7 +454,8 @@ __global__ void __launch_bounds__(NT) emit_kernel(Problem p, const __grid_consta
                                                   const mtx_meshlet_descriptor *__restrict__ desc,
                                                   const uint32_t *__restrict__ faces, void *__restrict__ vertices,
                                                   uint64_t vcap, uint32_t *__restrict__ indices, uint64_t tcap,
-                                                  uint32_t vfmt, uint32_t frame, uint32_t normals, DevStatus *st) {
+                                                  uint32_t vfmt, uint32_t frame, uint32_t normals,
+                                                  uint64_t block_cap, DevStatus *st) {
     extern __shared__ __align__(128) unsigned char smem[];
     const Plan pl = make_plan(p.B, sizeof(T), tma, true);
     uint32_t *rows = reinterpret_cast<uint32_t *>(smem + pl.off_rows);
@@ -467,6 +477,7 @@ __global__ void __launch_bounds__(NT) emit_kernel(Problem p, const __grid_consta
     }
     __syncthreads();
     const uint32_t count = *count_ptr;
+    if (count > block_cap) return;  // reported by the count pass
     const uint32_t B = p.B, BB = B * B, B1 = pl.B1;
     uint32_t phase = 0;
     const uint64_t nvert_cap = vcap, ntri_cap = tcap;
@@ -706,7 +717,7 @@ static mtx_status run_count(mtx_context *c, const Problem &p, const ExtractArgs 
     grid = std::max<uint64_t>(grid, 1);
     k<<<(unsigned)grid, NT, pl.bytes, s>>>(p, map, tma, a.ids, a.count, a.desc, a.desc_capacity, a.faces,
                                           a.count_status, &c->ctrl->count_ticket, a.totals, a.cell_cases,
-                                          &c->ctrl->status);
+                                          a.block_capacity, &c->ctrl->status);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "count launch");
     return MTX_OK;
@@ -725,7 +736,7 @@ static mtx_status run_emit(mtx_context *c, const Problem &p, const ExtractArgs &
     grid = std::max<uint64_t>(grid, 1);
     k<<<(unsigned)grid, NT, pl.bytes, s>>>(p, map, tma, a.ids, a.rank_map, a.count, a.desc, a.faces, a.vertices,
                                           a.vertex_capacity, a.indices, a.tri_capacity, a.vertex_format, a.frame,
-                                          a.normals, &c->ctrl->status);
+                                          a.normals, a.block_capacity, &c->ctrl->status);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "emit launch");
     return MTX_OK;

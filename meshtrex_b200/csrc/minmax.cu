@@ -11,6 +11,8 @@
 // the halo of block bz and the first slice of bz+1, so it is loaded once.
 // Only the halo row of the y direction is read twice, by two warps that run
 // side by side, so DRAM sees each voxel once and L2 serves the repeat.
+#include <algorithm>
+
 #include "mtx_internal.h"
 
 namespace mtx {
@@ -214,26 +216,50 @@ __global__ void __launch_bounds__(128) minmax_leaf_generic_kernel(const T *__res
     leaf[b] = make_uint2(mn, mx);
 }
 
-// One octree level: each texel reduces its up-to-8 children; children past
-// the source extent are skipped (minMaxOctreeReduce.comp.glsl:37-47).
-__global__ void __launch_bounds__(256) pyramid_level_kernel(const uint2 *__restrict__ src, uint32_t sx,
-                                                            uint32_t sy, uint32_t sz, uint2 *__restrict__ dst,
-                                                            uint32_t dx, uint32_t dy, uint32_t dz) {
-    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    uint64_t n = (uint64_t)dx * dy * dz;
-    if (i >= n) return;
-    uint32_t x = (uint32_t)(i % dx), y = (uint32_t)((i / dx) % dy), z = (uint32_t)(i / ((uint64_t)dx * dy));
-    uint32_t mn = ~0u, mx = 0u;
+// Three octree levels per launch: a CTA of 512 threads loads an 8x8x8 tile
+// of level l and writes the 4^3, 2^3 and 1 texels it covers in levels l+1..l+3
+// (each texel the min/max of its up-to-8 children; children past the level's
+// extent are skipped, minMaxOctreeReduce.comp.glsl:37-47).
+struct PyrLevels {
+    uint2 *base[4];      // level l .. l+3
+    uint32_t ext[4][3];  // their extents
+    int nout;            // levels written (1..3)
+};
+
+__global__ void __launch_bounds__(512) pyramid3_kernel(PyrLevels L, uint32_t tiles_x, uint32_t tiles_y) {
+    __shared__ uint2 s[512];
+    const uint32_t tx = blockIdx.x % tiles_x, ty = (blockIdx.x / tiles_x) % tiles_y, tz = blockIdx.x / (tiles_x * tiles_y);
+    const uint32_t lx = threadIdx.x & 7, ly = (threadIdx.x >> 3) & 7, lz = threadIdx.x >> 6;
+    const uint32_t x = tx * 8 + lx, y = ty * 8 + ly, z = tz * 8 + lz;
+    uint2 v = make_uint2(~0u, 0u);
+    if (x < L.ext[0][0] && y < L.ext[0][1] && z < L.ext[0][2])
+        v = L.base[0][((uint64_t)z * L.ext[0][1] + y) * L.ext[0][0] + x];
+    s[threadIdx.x] = v;
+    __syncthreads();
+    uint32_t n = 8;  // current tile edge in shared memory
+    for (int k = 1; k <= L.nout; ++k) {
+        const uint32_t m = n >> 1;
+        uint2 r = make_uint2(~0u, 0u);
+        const bool act = threadIdx.x < m * m * m;
+        const uint32_t cx = threadIdx.x % m, cy = (threadIdx.x / m) % m, cz = threadIdx.x / (m * m);
+        if (act) {
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {
-        uint32_t cx = 2 * x + (c & 1), cy = 2 * y + ((c >> 1) & 1), cz = 2 * z + (c >> 2);
-        if (cx < sx && cy < sy && cz < sz) {
-            uint2 v = src[((uint64_t)cz * sy + cy) * sx + cx];
-            mn = min(mn, v.x);
-            mx = max(mx, v.y);
+            for (int c = 0; c < 8; ++c) {
+                const uint2 w = s[((2 * cz + (c >> 2)) * n + 2 * cy + ((c >> 1) & 1)) * n + 2 * cx + (c & 1)];
+                r.x = min(r.x, w.x);
+                r.y = max(r.y, w.y);
+            }
         }
+        __syncthreads();
+        if (act) {
+            s[threadIdx.x] = r;  // compact m^3 layout for the next level
+            const uint32_t ox = tx * m + cx, oy = ty * m + cy, oz = tz * m + cz;
+            if (ox < L.ext[k][0] && oy < L.ext[k][1] && oz < L.ext[k][2])
+                L.base[k][((uint64_t)oz * L.ext[k][1] + oy) * L.ext[k][0] + ox] = r;
+        }
+        __syncthreads();
+        n = m;
     }
-    dst[i] = make_uint2(mn, mx);
 }
 
 // ------------------------------------------------------------------ host
@@ -289,12 +315,16 @@ mtx_status launch_minmax_leaf(mtx_context *c, const Problem &p, uint2 *leaf, cud
 
 mtx_status launch_pyramid(mtx_context *c, uint2 *all, int levels, const uint32_t ext[][3],
                           const uint64_t *offset, cudaStream_t s) {
-    for (int l = 1; l < levels; ++l) {
-        uint64_t n = (uint64_t)ext[l][0] * ext[l][1] * ext[l][2];
-        unsigned blocks = (unsigned)((n + 255) / 256);
-        pyramid_level_kernel<<<blocks, 256, 0, s>>>(all + offset[l - 1], ext[l - 1][0], ext[l - 1][1],
-                                                     ext[l - 1][2], all + offset[l], ext[l][0], ext[l][1],
-                                                     ext[l][2]);
+    for (int l = 0; l + 1 < levels; l += 3) {
+        PyrLevels P;
+        P.nout = std::min(3, levels - 1 - l);
+        for (int k = 0; k <= 3; ++k) {
+            const int lv = std::min(l + k, levels - 1);
+            P.base[k] = all + offset[lv];
+            for (int a = 0; a < 3; ++a) P.ext[k][a] = ext[lv][a];
+        }
+        const uint32_t tx = ceil_div(ext[l][0], 8), ty = ceil_div(ext[l][1], 8), tz = ceil_div(ext[l][2], 8);
+        pyramid3_kernel<<<tx * ty * tz, 512, 0, s>>>(P, tx, ty);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return cuda_fail(c, e, "pyramid launch");
     }

@@ -43,6 +43,7 @@ struct mtx_context {
     mtx::Ctrl *ctrl = nullptr;   // device
     uint32_t *pinned = nullptr;  // pinned host words for count readbacks
     mtx::Scratch filter_status, count_status, faces, leaf, ids, rank, desc, misc;
+    mtx_profiler *prof = nullptr;  // records stage times of calls given no profiler
 };
 
 namespace mtx {
@@ -107,6 +108,7 @@ struct ExtractArgs {
     mtx_meshlet_descriptor *desc;  // per active block {vbase, 3*tbase, nv, nt}
     uint64_t desc_capacity;
     uint32_t *faces;            // 3*B*B words per active block
+    uint64_t block_capacity;    // active blocks that desc/faces/count_status can hold
     uint64_t *count_status;     // look-back words, one per active block, zeroed
     uint32_t *totals;           // device uint32[4] {vertexCount, indexCount, meshletCount, activeCount}
     uint8_t *cell_cases;        // optional

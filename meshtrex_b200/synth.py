@@ -87,6 +87,7 @@ def _slabs(Z: int, Y: int, X: int, budget_voxels: int = 1 << 24):
 
 
 def _grids(z0, z1, Z, Y, X, device):
+    """Coordinate grids of slices z0..z1 of a [Z, Y, X] volume."""
     z = _coords(Z, device)[z0:z1].view(-1, 1, 1)
     y = _coords(Y, device).view(1, -1, 1)
     x = _coords(X, device).view(1, 1, -1)
@@ -140,16 +141,20 @@ def blobs(n: int = 256, seed: int = 0, device="cpu") -> torch.Tensor:
 
 
 # ---------------------------------------------------------------- fbm_ball
-def fbm_ball(n: int = 1024, seed: int = 1, device="cpu", shape_zyx=None) -> torch.Tensor:
-    """65535 * clamp(0.5 + 0.5 (0.35 - |x - 0.5|) / 0.35 + 0.08 fBm(5 oct, freq 4), 0, 1)."""
+def fbm_ball(n: int = 1024, seed: int = 1, device="cpu", shape_zyx=None, zslab=None) -> torch.Tensor:
+    """65535 * clamp(0.5 + 0.5 (0.35 - |x - 0.5|) / 0.35 + 0.08 fBm(5 oct, freq 4), 0, 1).
+
+    zslab=(za, zb) generates only slices za..zb of the full volume."""
     Z, Y, X = shape_zyx or (n, n, n)
-    out = torch.empty((Z, Y, X), dtype=torch.uint16, device=device)
-    for z0, z1 in _slabs(Z, Y, X, 1 << 23):
+    za, zb = zslab or (0, Z)
+    out = torch.empty((zb - za, Y, X), dtype=torch.uint16, device=device)
+    for s0, s1 in _slabs(zb - za, Y, X, 1 << 23):
+        z0, z1 = za + s0, za + s1
         x, y, z = _grids(z0, z1, Z, Y, X, device)
         r = torch.sqrt((x - 0.5) ** 2 + (y - 0.5) ** 2 + (z - 0.5) ** 2)
         xb, yb, zb = torch.broadcast_tensors(x, y, z)
         f = 0.5 + 0.5 * (0.35 - r) / 0.35 + 0.08 * fbm(xb, yb, zb, 5, 4.0, seed)
-        out[z0:z1] = _to_dtype(65535.0 * torch.clamp(f, 0.0, 1.0), torch.uint16)
+        out[s0:s1] = _to_dtype(65535.0 * torch.clamp(f, 0.0, 1.0), torch.uint16)
     return out
 
 
