@@ -274,6 +274,18 @@ uint32_t mtx_profiler_region_count(mtx_profiler_t prof);
 /* name (<= 63 chars + NUL) and the last frame's and running-average time in ms. */
 mtx_status mtx_profiler_region(mtx_profiler_t prof, uint32_t i, char name[64], double *last_ms,
                                double *avg_ms, uint32_t *frames);
+/* Launch-shape knobs of the kernels (0 = built-in default), the search space
+ * of mtx_autotune; meshtrex's only counterparts are its compile-time
+ * workgroup sizes and specialization constants (extractionPipeline.cpp:238-256). */
+typedef struct mtx_tuning {
+    uint32_t minmaxZChunk;  /* block slabs per warp in the min/max pass */
+    uint32_t minmaxSlices;  /* z slices whose loads are issued together: 1, 2 (default) or 4 */
+    uint32_t extractWarps;  /* warps per CTA of the extraction passes: 1, 2, 4 (default) or 8 */
+    uint32_t staging;       /* mtx_staging used when the extract options say AUTO */
+} mtx_tuning;
+mtx_status mtx_context_set_tuning(mtx_context_t ctx, const mtx_tuning *t);
+mtx_status mtx_context_get_tuning(mtx_context_t ctx, mtx_tuning *t);
+
 /* Records the stage times of every later call on this context that is not
  * given its own profiler, the asynchronous whole-path call included (NULL
  * turns it off); the GPUProfiler* argument of meshtrex's managers made

@@ -76,6 +76,11 @@ class ExtractionOutput(C.Structure):
                 ("vertexStride", C.c_uint32)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("minmaxZChunk", C.c_uint32), ("minmaxSlices", C.c_uint32),
+                ("extractWarps", C.c_uint32), ("staging", C.c_uint32)]
+
+
 class MeshBuffers(C.Structure):
     _fields_ = [("vertices", C.c_void_p), ("vertexCapacity", C.c_uint64),
                 ("indices", C.c_void_p), ("triangleCapacity", C.c_uint64),
@@ -117,6 +122,8 @@ SIGNATURES = [
                                       C.POINTER(ExtractOptions), C.POINTER(MeshBuffers)]),
     ("mtx_profiler_create", _ST, [_P, C.POINTER(_P)]),
     ("mtx_context_set_profiler", _ST, [_P, _P]),
+    ("mtx_context_set_tuning", _ST, [_P, C.POINTER(Tuning)]),
+    ("mtx_context_get_tuning", _ST, [_P, C.POINTER(Tuning)]),
     ("mtx_profiler_destroy", _ST, [_P]),
     ("mtx_profiler_begin_frame", _ST, [_P]),
     ("mtx_profiler_end_frame", _ST, [_P]),

@@ -66,6 +66,16 @@ class Context:
         L.check(L.lib().mtx_context_set_profiler(self.handle, prof.handle if prof else None),
                 "mtx_context_set_profiler")
 
+    def set_tuning(self, minmax_zchunk=0, minmax_slices=0, extract_warps=0, staging=0):
+        t = L.Tuning(minmax_zchunk, minmax_slices, extract_warps, staging)
+        L.check(L.lib().mtx_context_set_tuning(self.handle, C.byref(t)), "mtx_context_set_tuning",
+                self.handle)
+
+    def get_tuning(self) -> dict:
+        t = L.Tuning()
+        L.check(L.lib().mtx_context_get_tuning(self.handle, C.byref(t)), "mtx_context_get_tuning")
+        return {f: getattr(t, f) for f, _ in L.Tuning._fields_}
+
     def fail_allocation(self, k: int):
         L.check(L.lib().mtx_debug_fail_allocation(self.handle, k), "mtx_debug_fail_allocation")
 

@@ -531,7 +531,6 @@ mtx_status mtx_extract_meshlet_descriptors(mtx_context_t c, const mtx_minmax_out
         return s;
     };
     if ((r = scratch_reserve(c, c->faces, (size_t)n * 3 * B * B * 4)) != MTX_OK) return bail(r);
-    if ((r = scratch_reserve(c, c->count_status, (size_t)n * 8)) != MTX_OK) return bail(r);
 
     ExtractArgs a;
     memset(&a, 0, sizeof(a));
@@ -567,7 +566,7 @@ mtx_status mtx_extract_meshlet_descriptors(mtx_context_t c, const mtx_minmax_out
     out->vertexBuffer = {vb, (uint64_t)V * out->vertexStride};
     if ((r = dev_alloc(c, &ib, (size_t)I * 4)) != MTX_OK) return bail(r);
     out->indexBuffer = {ib, (uint64_t)I * 4};
-    a.vertices = vb;
+    a.vertices = vb;  // sizes are known only now
     a.vertex_capacity = V;
     a.indices = (uint32_t *)ib;
     a.tri_capacity = I / 3;
@@ -625,7 +624,6 @@ mtx_status mtx_extract_plain_async(mtx_context_t c, const mtx_volume *vol, const
     if ((r = scratch_reserve(c, c->leaf, texels * 8)) != MTX_OK) return r;
     if ((r = scratch_reserve(c, c->ids, p.nblocks * 4)) != MTX_OK) return r;
     if ((r = scratch_reserve(c, c->rank, p.nblocks * 4)) != MTX_OK) return r;
-    if ((r = scratch_reserve(c, c->count_status, p.nblocks * 8)) != MTX_OK) return r;
     if ((r = scratch_reserve(c, c->faces, maxa * 3 * B * B * 4)) != MTX_OK) return r;
     mtx_meshlet_descriptor *desc = out->meshlets;
     uint64_t dcap = out->meshletCapacity;
@@ -648,7 +646,7 @@ mtx_status mtx_extract_plain_async(mtx_context_t c, const mtx_volume *vol, const
     }
     prof_begin(P, "Active_Block_Filtering", s);
     r = launch_filter(c, p, (const uint2 *)c->leaf.ptr, (uint32_t *)c->ids.ptr, (uint32_t *)c->rank.ptr,
-                      &c->ctrl->active_count, (uint64_t *)c->count_status.ptr, s);
+                      &c->ctrl->active_count, nullptr, s);
     prof_end(P, s);
     if (r != MTX_OK) return r;
     ExtractArgs a;
@@ -697,6 +695,22 @@ mtx_status mtx_profiler_create(mtx_context_t c, mtx_profiler_t *out) {
     if (!p) return MTX_ERR_OOM;
     p->ctx = c;
     *out = p;
+    return MTX_OK;
+}
+
+mtx_status mtx_context_set_tuning(mtx_context_t c, const mtx_tuning *t) {
+    if (!c || !t) return MTX_ERR_INVALID_ARG;
+    if (t->minmaxSlices > 4 || t->minmaxSlices == 3 || t->staging > MTX_STAGING_LDG ||
+        (t->extractWarps && t->extractWarps != 1 && t->extractWarps != 2 && t->extractWarps != 4 &&
+         t->extractWarps != 8))
+        return fail(c, MTX_ERR_INVALID_ARG, "bad tuning values");
+    c->tuning = *t;
+    return MTX_OK;
+}
+
+mtx_status mtx_context_get_tuning(mtx_context_t c, mtx_tuning *t) {
+    if (!c || !t) return MTX_ERR_INVALID_ARG;
+    *t = c->tuning;
     return MTX_OK;
 }
 

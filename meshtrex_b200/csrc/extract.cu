@@ -2,25 +2,29 @@
 // (meshtrex: marching_cubes_pmb.task.glsl:101-216 and
 // marching_cubes_pmb.mesh.glsl:185-393, drawn by extractionManager.cpp:638-640).
 //
-// Two persistent kernels over the compacted block list:
+// One warp owns one active block at a time; a CTA runs several such warps
+// that share only the case tables.  Each warp double-buffers the (B+1)^3
+// voxel tile of its block in shared memory (a TMA 3D tile, or plain loads
+// when the volume's rows are not 16-byte aligned), so the next block's tile
+// is in flight while the current one is processed.
 //
-//  count  stages the block's (B+1)^3 voxels in shared memory (a TMA 3D tile
-//         or plain loads), turns every voxel row into an inside bitmask, and
-//         from those bitmasks gets, per row, the crossed +x/+y/+z edges each
-//         voxel owns (PMB ownership) and the case index of each cell.  It
-//         scans the per-block vertex/triangle counts across blocks with a
-//         decoupled look-back (blocks taken in rank order by ticket), and
-//         records for the block's three low faces the vertex prefix and edge
-//         mask of every face voxel: that is all a neighbouring block needs to
-//         name this block's vertices.
-//  emit   restages the tile, rebuilds the masks, writes each owned vertex
-//         once at its final index, and writes triangles whose vertex ids come
-//         from a shared table of the (B+1)^3 context: own voxels from the row
-//         prefixes, the +x/+y/+z layer from the neighbours' face records.
+//  count pass   (blocks taken by ticket, i.e. in rank order)
+//     voxel rows -> inside bitmasks -> per-row crossed +x/+y/+z edges owned
+//     by each voxel (PMB ownership) and per-cell case indices -> the block's
+//     vertex and triangle counts -> decoupled look-back over ranks -> the
+//     block's first vertex and triangle -> writes its vertices (each exactly
+//     once, staged 32 voxels at a time and stored coalesced), its meshlet
+//     descriptor and, for its three low faces, the vertex prefix and edge
+//     mask of every face voxel: all a neighbouring block needs to name them.
+//  triangle pass
+//     rebuilds the masks, gathers the +x/+y/+z layer's vertex ids from the
+//     neighbours' face records, and emits triangles 32 cells at a time:
+//     warp scan of the per-cell triangle counts, indices staged in shared
+//     memory, coalesced stores.
 //
-// Output order is canonical (and equals the CPU oracle's): vertices by
-// (block rank, owner voxel x-fastest in the block, axis x<y<z); triangles by
-// (block rank, cell x-fastest in the block, triangle number in the case).
+// Output order is canonical and equals the CPU oracle's: vertices by (block
+// rank, owner voxel x-fastest in the block, axis x<y<z); triangles by (block
+// rank, cell x-fastest in the block, triangle number in the case).
 #include <algorithm>
 
 #include "mtx_internal.h"
@@ -30,58 +34,83 @@ namespace mtx {
 __constant__ uint64_t c_mc_cases[256];
 __constant__ uint8_t c_mc_owner[12];
 
-// ------------------------------------------------------------- smem plan
-struct Plan {
-    uint32_t B, B1, PX;        // block edge, B+1, tile row pitch (elements)
-    uint32_t off_tile, off_rows, off_cross, off_vp, off_tp, off_vid, off_vm, off_tab, off_misc;
-    uint32_t bytes;
-    uint32_t tile_bytes;       // TMA transaction size
-};
+constexpr uint32_t kNoVertex = 0xffffffffu;
+// packed cases (2048 B), triangle counts (256 B), owners (16 B), rounded up so
+// that every warp's region -- and the TMA tile at its start -- is 128-byte aligned
+constexpr uint32_t kTableBytes = 2432;
+static_assert(kTableBytes % 128 == 0 && kTableBytes >= 2048 + 256 + 16, "table region must keep warp regions aligned");
+constexpr uint32_t kStageWords = 32 * 3;           // one batch: 32 triangles x 3 indices or 32 xyz
+constexpr uint32_t kJobWin = 256;                   // jobs (vertices or triangles) resolved per window
+constexpr int kMaxWarps = 8;                        // warps per CTA of the extraction kernels
 
 __host__ __device__ inline uint32_t align_up(uint32_t v, uint32_t a) { return (v + a - 1) / a * a; }
 
-__host__ __device__ inline Plan make_plan(uint32_t B, uint32_t esz, bool tma, bool emit) {
-    Plan p{};
+// ------------------------------------------------------- per-warp smem plan
+struct WPlan {
+    uint32_t B, B1, BB, PX, nbuf, nb3;
+    uint32_t rB, rB1, rBB;  // ceil(2^32 / d) reciprocals: n / d == __umulhi(n, r) for the sizes used here
+    uint32_t R;             // block rows walked per round of 32 lanes (32 / B)
+    uint32_t off_tile[2], off_bar, off_rows, off_cross, off_vp, off_tp, off_nvid, off_nm, off_stage, off_jobs;
+    uint32_t bytes;       // per warp
+    uint32_t tile_bytes;  // one tile (the TMA transaction size)
+};
+
+__host__ __device__ inline uint32_t tile_pitch(uint32_t B, uint32_t esz, bool tma) {
+    if (!tma) return B + 1;
+    const uint32_t A = 16 / esz;  // elements per 16 bytes
+    uint32_t g = 1;
+    for (uint32_t d = 1; d <= A; ++d)
+        if (B % d == 0 && A % d == 0) g = d;
+    const uint32_t xoff_max = (B % A == 0) ? 0 : A - g;
+    return align_up(xoff_max + B + 1, A);
+}
+
+__host__ __device__ inline WPlan make_wplan(uint32_t B, uint32_t esz, bool tma, bool tri_pass) {
+    WPlan p{};
     p.B = B;
     p.B1 = B + 1;
-    const uint32_t A = 16 / esz;  // elements per 16 bytes
-    if (tma) {
-        uint32_t g = 1;
-        for (uint32_t d = 1; d <= A; ++d)
-            if (B % d == 0 && A % d == 0) g = d;
-        uint32_t xoff_max = (B % A == 0) ? 0 : A - g;
-        p.PX = align_up(xoff_max + B + 1, A);
-    } else {
-        p.PX = B + 1;
-    }
-    uint32_t o = 0;
-    p.off_tile = o;
+    p.BB = B * B;
+    p.nb3 = 3 * B * B + 3 * B + 1;  // voxels of the (B+1)^3 context outside the block
+    p.rB = (uint32_t)((0x100000000ull + B - 1) / B);
+    p.rB1 = (uint32_t)((0x100000000ull + B) / (B + 1));
+    p.rBB = (uint32_t)((0x100000000ull + B * B - 1) / (B * B));
+    p.R = 32 / B;
+    p.PX = tile_pitch(B, esz, tma);
     p.tile_bytes = p.PX * p.B1 * p.B1 * esz;
-    o = align_up(o + p.tile_bytes, 128);
-    p.off_rows = o;                       // (B+1)^2 inside masks
-    o = align_up(o + 4 * p.B1 * p.B1, 16);
-    p.off_cross = o;                      // 3 * B^2 crossing masks
-    o = align_up(o + 12 * B * B, 16);
-    p.off_vp = o;                         // B^2 vertex prefixes (per owned row)
-    o = align_up(o + 4 * B * B, 16);
-    p.off_tp = o;                         // B^2 triangle prefixes (per cell row)
-    o = align_up(o + 4 * B * B, 16);
-    if (emit) {
-        p.off_vid = o;                    // (B+1)^3 first-vertex ids
-        o = align_up(o + 4 * p.B1 * p.B1 * p.B1, 16);
-        p.off_vm = o;                     // (B+1)^3 owned-edge masks
-        o = align_up(o + p.B1 * p.B1 * p.B1, 16);
-        p.off_tab = o;                    // packed case table
-        o = align_up(o + 8 * 256, 16);
-    } else {
-        p.off_tab = o;                    // triangle counts only
-        o = align_up(o + 256, 16);
+    p.nbuf = p.tile_bytes <= 4096 ? 2 : 1;
+    uint32_t o = 0;
+    for (uint32_t b = 0; b < 2; ++b) {
+        p.off_tile[b] = o;
+        if (b < p.nbuf) o = align_up(o + p.tile_bytes, 128);
     }
-    p.off_misc = o;                       // scan scratch, neighbour info, mbarrier
-    o += 512;
+    if (p.nbuf == 1) p.off_tile[1] = p.off_tile[0];
+    p.off_bar = o;
+    o += 16;
+    p.off_rows = o;
+    o = align_up(o + 4 * p.B1 * p.B1, 16);
+    p.off_cross = o;
+    o = align_up(o + 12 * p.BB, 16);
+    p.off_vp = o;
+    o = align_up(o + 4 * p.BB, 16);
+    p.off_tp = o;
+    o = align_up(o + 4 * p.BB, 16);
+    if (tri_pass) {
+        p.off_nvid = o;
+        o = align_up(o + 4 * p.nb3, 16);
+        p.off_nm = o;
+        o = align_up(o + p.nb3, 16);
+    }
+    p.off_stage = o;
+    o = align_up(o + 4 * kStageWords, 16);
+    p.off_jobs = o;  // a window of packed jobs (triangles or vertices) in output order
+    o = align_up(o + 4 * kJobWin, 16);
     p.bytes = align_up(o, 128);
     return p;
 }
+
+// n / d and n % d for the block-local sizes (n < 70000, 2 <= d < 300), exact.
+__device__ __forceinline__ uint32_t fdiv(uint32_t n, uint32_t r) { return __umulhi(n, r); }
+__device__ __forceinline__ uint32_t fmod(uint32_t n, uint32_t r, uint32_t d) { return n - __umulhi(n, r) * d; }
 
 struct Geo {
     uint32_t ox, oy, oz;  // block origin (voxels)
@@ -90,76 +119,128 @@ struct Geo {
     uint32_t xoff;        // tile column of the block's first voxel
 };
 
-__device__ __forceinline__ Geo block_geo(uint32_t id, uint32_t B, uint32_t GX, uint32_t GY, uint32_t X, bool tma,
-                                         uint32_t esz) {
+__device__ __forceinline__ Geo block_geo(uint32_t id, const Problem &p, bool tma, uint32_t esz) {
     Geo g;
-    g.bx = id % GX;
-    g.by = (id / GX) % GY;
-    g.bz = id / (GX * GY);
-    g.ox = g.bx * B;
-    g.oy = g.by * B;
-    g.oz = g.bz * B;
-    g.nx = min(B, X - g.ox);
-    const uint32_t A = 16 / esz;
-    g.xoff = tma ? (g.ox % A) : 0u;
+    g.bx = id % p.GX;
+    g.by = (id / p.GX) % p.GY;
+    g.bz = id / (p.GX * p.GY);
+    g.ox = g.bx * p.B;
+    g.oy = g.by * p.B;
+    g.oz = g.bz * p.B;
+    g.nx = min(p.B, p.X - g.ox);
+    g.xoff = tma ? (g.ox % (16 / esz)) : 0u;
     return g;
 }
 
-// Stage the (B+1)^3 voxels at the block origin into the tile.  TMA fills
-// voxels outside the volume with zeros; plain loads do the same explicitly.
-template <typename T>
-__device__ __forceinline__ bool stage_tile(const Problem &p, const CUtensorMap *map, const Plan &pl, const Geo &g,
-                                           unsigned char *smem, uint64_t *bar, uint32_t &phase, bool tma,
-                                           DevStatus *st) {
-    T *tile = reinterpret_cast<T *>(smem + pl.off_tile);
-    if (tma) {
-        if (threadIdx.x == 0) {
-            mbar_arrive_expect_tx(bar, pl.tile_bytes);
-            tma_load_3d(tile, map, bar, (int)(g.ox - g.xoff), (int)g.oy, (int)g.oz);
-        }
-        const bool ok = mbar_wait_bounded(bar, phase);
-        phase ^= 1u;
-        // every thread must take the same branch before the next barrier
-        if (__syncthreads_or(!ok)) {
-            if (threadIdx.x == 0) report(st, MTX_ERR_TIMEOUT, kSiteTmaWait, g.ox, g.oy);
+// ----------------------------------------------------------- warp tiles
+// Starts the load of a block's (B+1)^3 tile into buffer `buf`.  TMA: lane 0
+// issues one cp.async.bulk.tensor (zero fill outside the volume).  Plain
+// loads are done in tile_wait instead.
+template <typename T, bool TMA>
+__device__ __forceinline__ void tile_issue(const WPlan &pl, unsigned char *ws, uint32_t buf, const Geo &g,
+                                           const CUtensorMap *map) {
+    if (!TMA) return;
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0) {
+        uint64_t *bar = reinterpret_cast<uint64_t *>(ws + pl.off_bar) + buf;
+        fence_proxy_async();  // earlier generic reads of this buffer come first
+        mbar_arrive_expect_tx(bar, pl.tile_bytes);
+        tma_load_3d(ws + pl.off_tile[buf], map, bar, (int)(g.ox - g.xoff), (int)g.oy, (int)g.oz);
+    }
+}
+
+template <typename T, bool TMA>
+__device__ __forceinline__ bool tile_wait(const Problem &p, const WPlan &pl, unsigned char *ws, uint32_t buf,
+                                          const Geo &g, uint32_t &parity, DevStatus *st) {
+    if (TMA) {
+        uint64_t *bar = reinterpret_cast<uint64_t *>(ws + pl.off_bar) + buf;
+        const bool ok = mbar_wait_bounded(bar, (parity >> buf) & 1u);
+        if (!__all_sync(0xffffffffu, ok)) {
+            if ((threadIdx.x & 31) == 0) report(st, MTX_ERR_TIMEOUT, kSiteTmaWait, g.ox, g.oy);
+            // give the copy in flight one more bounded wait before the warp leaves
+            mbar_wait_bounded(bar, (parity >> buf) & 1u);
+            parity ^= 1u << buf;
             return false;
         }
+        parity ^= 1u << buf;
         return true;
     }
+    T *tile = reinterpret_cast<T *>(ws + pl.off_tile[buf]);
     const T *vol = reinterpret_cast<const T *>(p.vol);
     const uint32_t n = pl.B1 * pl.B1 * pl.B1;
-    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) {
-        uint32_t x = i % pl.B1, y = (i / pl.B1) % pl.B1, z = i / (pl.B1 * pl.B1);
-        uint32_t gx = g.ox + x, gy = g.oy + y, gz = g.oz + z;
+    for (uint32_t i = threadIdx.x & 31; i < n; i += 32) {
+        const uint32_t iq = fdiv(i, pl.rB1);
+        const uint32_t x = i - iq * pl.B1, z = fdiv(iq, pl.rB1), y = iq - z * pl.B1;
+        const uint32_t gx = g.ox + x, gy = g.oy + y, gz = g.oz + z;
         T v = T(0);
         if (gx < p.X && gy < p.Y && gz < p.Z) v = __ldg(vol + ((uint64_t)gz * p.Y + gy) * p.X + gx);
         tile[(z * pl.B1 + y) * pl.PX + x] = v;
     }
-    __syncthreads();
+    __syncwarp();
     return true;
 }
 
-// Inside bitmask of every tile row (bit x <=> voxel at or below iso and in the volume).
+// Waits (bounded) for a prefetched tile that will not be used, so that no
+// copy into this warp's shared memory is in flight when it leaves.
+template <bool TMA>
+__device__ __forceinline__ void tile_drain(const WPlan &pl, unsigned char *ws, uint32_t buf, uint32_t &parity) {
+    if (!TMA) return;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(ws + pl.off_bar) + buf;
+    mbar_wait_bounded(bar, (parity >> buf) & 1u);
+    parity ^= 1u << buf;
+}
+
+// Inside bitmask of every tile row: bit x <=> voxel at or below iso and inside
+// the volume.  Integer voxels compare against floor(iso); rows that start on a
+// 4-byte boundary are tested 2 (uint16) or 4 (uint8) voxels per instruction.
 template <typename T>
-__device__ __forceinline__ void row_masks(const Problem &p, const Plan &pl, const Geo &g, unsigned char *smem) {
-    const T *tile = reinterpret_cast<const T *>(smem + pl.off_tile);
-    uint32_t *rows = reinterpret_cast<uint32_t *>(smem + pl.off_rows);
-    const uint32_t nrows = pl.B1 * pl.B1;
-    const uint32_t xin = min(pl.B1, p.X - g.ox);  // voxels of the row inside the volume
-    for (uint32_t q = threadIdx.x; q < nrows; q += blockDim.x) {
-        uint32_t y = q % pl.B1, z = q / pl.B1;
+__device__ __forceinline__ void build_rows(const Problem &p, const WPlan &pl, unsigned char *ws, uint32_t buf,
+                                           const Geo &g) {
+    const T *tile = reinterpret_cast<const T *>(ws + pl.off_tile[buf]);
+    uint32_t *rows = reinterpret_cast<uint32_t *>(ws + pl.off_rows);
+    const uint32_t xin = min(pl.B1, p.X - g.ox);
+    const uint32_t xmask = (1u << xin) - 1u;  // xin <= 17
+    // integer voxels: value <= iso  <=>  value <= floor(iso) (never when iso < 0 or NaN)
+    const bool never = !(p.iso >= 0.0f);
+    const uint32_t thr = never ? 0u : (uint32_t)fminf(floorf(p.iso), sizeof(T) == 1 ? 255.0f : 65535.0f);
+    const bool simd = Vox<T>::code != 2 && ((pl.PX * sizeof(T)) % 4 == 0) && ((g.xoff * sizeof(T)) % 4 == 0);
+    for (uint32_t q = threadIdx.x & 31; q < pl.B1 * pl.B1; q += 32) {
+        const uint32_t z = fdiv(q, pl.rB1), y = q - z * pl.B1;
         uint32_t m = 0;
         if (g.oy + y < p.Y && g.oz + z < p.Z) {
             const T *r = tile + (z * pl.B1 + y) * pl.PX + g.xoff;
-            for (uint32_t x = 0; x < xin; ++x) m |= (Vox<T>::val(r[x]) <= p.iso ? 1u : 0u) << x;
+            if (Vox<T>::code == 2) {
+                for (uint32_t x = 0; x < xin; ++x) m |= (Vox<T>::val(r[x]) <= p.iso ? 1u : 0u) << x;
+            } else if (never) {
+                m = 0;
+            } else if (simd && sizeof(T) == 2) {
+                const uint32_t *w = reinterpret_cast<const uint32_t *>(r);
+                const uint32_t t2 = thr | (thr << 16);
+                for (uint32_t i = 0; 2 * i < xin; ++i) {
+                    const uint32_t c = __vcmpleu2(w[i], t2) & 0x00010001u;
+                    m |= ((c | (c >> 15)) & 3u) << (2 * i);
+                }
+                m &= xmask;
+            } else if (simd && sizeof(T) == 1) {
+                const uint32_t *w = reinterpret_cast<const uint32_t *>(r);
+                const uint32_t t4 = thr * 0x01010101u;
+                for (uint32_t i = 0; 4 * i < xin; ++i) {
+                    const uint32_t c = __vcmpleu4(w[i], t4) & 0x01010101u;
+                    m |= ((c * 0x01020408u) >> 24) << (4 * i);
+                }
+                m &= xmask;
+            } else {
+                for (uint32_t x = 0; x < xin; ++x) m |= ((uint32_t)r[x] <= thr ? 1u : 0u) << x;
+            }
         }
         rows[q] = m;
     }
+    __syncwarp();
 }
 
-// Crossing masks of the owned voxel row (y, z): bit x of Xc/Yc/Zc set when
-// the owned +x/+y/+z edge of voxel (x, y, z) is cut.
-__device__ __forceinline__ void row_cross(const Problem &p, const Plan &pl, const Geo &g, const uint32_t *rows,
+// Crossing masks of owned voxel row (y, z) (bit x of xc/yc/zc: the +x/+y/+z
+// edge owned by voxel (x, y, z) is cut) from the inside bitmasks.
+__device__ __forceinline__ void row_cross(const Problem &p, const WPlan &pl, const Geo &g, const uint32_t *rows,
                                           uint32_t y, uint32_t z, uint32_t &xc, uint32_t &yc, uint32_t &zc) {
     xc = yc = zc = 0;
     if (g.oy + y >= p.Y || g.oz + z >= p.Z) return;
@@ -172,238 +253,116 @@ __device__ __forceinline__ void row_cross(const Problem &p, const Plan &pl, cons
     if (g.oz + z + 1 < p.Z) zc = (r0 ^ rows[(z + 1) * pl.B1 + y]) & own;
 }
 
-__device__ __forceinline__ uint32_t cell_case(uint32_t r00, uint32_t r01, uint32_t r10, uint32_t r11, uint32_t x) {
-    // corners (marching_cubes_pmb.mesh.glsl:84-93): r00 = row (y,z), r01 = (y+1,z),
-    // r10 = (y,z+1), r11 = (y+1,z+1)
-    return ((r00 >> x) & 1u) | (((r00 >> (x + 1)) & 1u) << 1) | (((r01 >> (x + 1)) & 1u) << 2) |
-           (((r01 >> x) & 1u) << 3) | (((r10 >> x) & 1u) << 4) | (((r10 >> (x + 1)) & 1u) << 5) |
-           (((r11 >> (x + 1)) & 1u) << 6) | (((r11 >> x) & 1u) << 7);
+// Case index of the cell at (x, y, z) from the inside bitmasks (corner order
+// of marching_cubes_pmb.mesh.glsl:84-93: r00 = row (y,z), r01 = (y+1,z),
+// r10 = (y,z+1), r11 = (y+1,z+1)).
+__device__ __forceinline__ uint32_t cell_case(const uint32_t *rows, uint32_t B1, uint32_t x, uint32_t y, uint32_t z) {
+    const uint32_t r00 = rows[z * B1 + y] >> x, r01 = rows[z * B1 + y + 1] >> x;
+    const uint32_t r10 = rows[(z + 1) * B1 + y] >> x, r11 = rows[(z + 1) * B1 + y + 1] >> x;
+    return (r00 & 1u) | (r00 & 2u) | ((r01 & 2u) << 1) | ((r01 & 1u) << 3) | ((r10 & 1u) << 4) |
+           ((r10 & 2u) << 4) | ((r11 & 2u) << 5) | ((r11 & 1u) << 7);
 }
 
-// Number of cells of row (y, z) that lie inside the volume (0 if the row does not).
-__device__ __forceinline__ uint32_t cells_in_row(const Problem &p, const Plan &pl, const Geo &g, uint32_t y,
-                                                 uint32_t z) {
+// Whether the cell at (x, y, z) of the block lies inside the volume.
+__device__ __forceinline__ bool cell_valid(const Problem &p, const Geo &g, uint32_t x, uint32_t y, uint32_t z) {
+    return g.ox + x + 1 < p.X && g.oy + y + 1 < p.Y && g.oz + z + 1 < p.Z;
+}
+
+__device__ __forceinline__ uint32_t warp_excl_scan(uint32_t v, uint32_t &total) {
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= (uint32_t)o) x += y;
+    }
+    total = __shfl_sync(0xffffffffu, x, 31);
+    return x - v;
+}
+
+// Cells x of cell row (y, z) whose case is neither 0 nor 255 (bit x set), and
+// those that are entirely inside (all 8 corners at or below iso).
+__device__ __forceinline__ uint32_t mixed_cells(const Problem &p, const WPlan &pl, const Geo &g, const uint32_t *rows,
+                                                uint32_t y, uint32_t z, uint32_t &all_inside) {
+    all_inside = 0;
     if (g.oy + y + 1 >= p.Y || g.oz + z + 1 >= p.Z || g.ox + 1 >= p.X) return 0;
-    return min(pl.B, p.X - 1 - g.ox);
+    const uint32_t ncell = min(pl.B, p.X - 1 - g.ox), B1 = pl.B1;
+    const uint32_t cells = (1u << ncell) - 1u;
+    const uint32_t r00 = rows[z * B1 + y], r01 = rows[z * B1 + y + 1];
+    const uint32_t r10 = rows[(z + 1) * B1 + y], r11 = rows[(z + 1) * B1 + y + 1];
+    const uint32_t all = r00 & r01 & r10 & r11, any = r00 | r01 | r10 | r11;
+    all_inside = all & (all >> 1) & cells;
+    return (any | (any >> 1)) & ~(all & (all >> 1)) & cells;
 }
 
-// ------------------------------------------------------------- count pass
-constexpr uint64_t kCnt31 = 0x7fffffffull;
-
-template <typename T, int NT>
-__global__ void __launch_bounds__(NT) count_kernel(Problem p, const __grid_constant__ CUtensorMap map, bool tma,
-                                                   const uint32_t *__restrict__ ids,
-                                                   const uint32_t *__restrict__ count_ptr,
-                                                   mtx_meshlet_descriptor *__restrict__ desc,
-                                                   uint64_t desc_capacity, uint32_t *__restrict__ faces,
-                                                   uint64_t *status, uint32_t *ticket, uint32_t *totals,
-                                                   uint8_t *__restrict__ cell_cases, uint64_t block_cap,
-                                                   DevStatus *st) {
-    extern __shared__ __align__(128) unsigned char smem[];
-    const Plan pl = make_plan(p.B, sizeof(T), tma, false);
-    uint32_t *rows = reinterpret_cast<uint32_t *>(smem + pl.off_rows);
-    uint32_t *cross = reinterpret_cast<uint32_t *>(smem + pl.off_cross);
-    uint32_t *vp = reinterpret_cast<uint32_t *>(smem + pl.off_vp);
-    uint32_t *tp = reinterpret_cast<uint32_t *>(smem + pl.off_tp);
-    uint8_t *ntab = smem + pl.off_tab;
-    uint32_t *misc = reinterpret_cast<uint32_t *>(smem + pl.off_misc);
-    uint64_t *misc64 = reinterpret_cast<uint64_t *>(smem + pl.off_misc);
-    // misc layout: [0..15] u64 scan scratch, [32] u32 rank, [33] abort, [34..35] u64 prefix, bar at +448
-    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + pl.off_misc + 448);
-
-    for (uint32_t i = threadIdx.x; i < 256; i += NT) ntab[i] = (uint8_t)(c_mc_cases[i] & 0xFu);
-    if (threadIdx.x == 0 && tma) {
-        mbar_init(bar, 1);
-        fence_mbar_init();
+// Per-row crossing masks, vertex prefixes and (want_tris) triangle prefixes,
+// and the block's vertex/triangle counts.  Lane l owns rows [l*R, l*R + R) so
+// that the row prefixes follow from one warp scan.  Optionally writes the
+// per-cell case bytes.
+__device__ __forceinline__ void block_counts(const Problem &p, const WPlan &pl, unsigned char *ws, const Geo &g,
+                                             const uint8_t *ntab, bool want_tris, uint8_t *cases_out,
+                                             uint32_t &nv, uint32_t &nt) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t *rows = reinterpret_cast<const uint32_t *>(ws + pl.off_rows);
+    uint32_t *cross = reinterpret_cast<uint32_t *>(ws + pl.off_cross);
+    uint32_t *vp = reinterpret_cast<uint32_t *>(ws + pl.off_vp);
+    uint32_t *tp = reinterpret_cast<uint32_t *>(ws + pl.off_tp);
+    const uint32_t B = pl.B, BB = pl.BB;
+    const uint32_t R = (BB + 31) / 32;
+    uint32_t sv = 0, stri = 0;
+    for (uint32_t k = 0; k < R; ++k) {
+        const uint32_t q = lane * R + k;
+        if (q >= BB) break;
+        const uint32_t z = fdiv(q, pl.rB), y = q - z * B;
+        uint32_t xc, yc, zc;
+        row_cross(p, pl, g, rows, y, z, xc, yc, zc);
+        cross[q] = xc;
+        cross[BB + q] = yc;
+        cross[2 * BB + q] = zc;
+        vp[q] = sv;  // lane-local prefixes, rebased below
+        sv += __popc(xc) + __popc(yc) + __popc(zc);
+        if (want_tris) {
+            tp[q] = stri;
+            uint32_t inside;
+            uint32_t mm = mixed_cells(p, pl, g, rows, y, z, inside);
+            if (cases_out)
+                for (uint32_t x = 0; x < B; ++x) cases_out[q * B + x] = ((inside >> x) & 1u) ? 255 : 0;
+            while (mm) {
+                const uint32_t x = __ffs(mm) - 1;
+                mm &= mm - 1u;
+                const uint32_t cfg = cell_case(rows, pl.B1, x, y, z);
+                stri += ntab[cfg];
+                if (cases_out) cases_out[q * B + x] = (uint8_t)cfg;
+            }
+        }
     }
-    if (tma && threadIdx.x == 0) prefetch_tensormap(&map);
-    __syncthreads();
-    const uint32_t count = *count_ptr;
-    const uint32_t B = p.B, BB = B * B;
-    uint32_t phase = 0;
-    if (count > block_cap || count > desc_capacity) {
-        // scratch sized for fewer active blocks: report the needed count, do nothing
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
-            report(st, MTX_ERR_CAPACITY, kSiteEmitCapacity, count, 3);
-            totals[3] = count;
-        }
-        return;
+    uint32_t tv, tt;
+    const uint32_t pv = warp_excl_scan(sv, tv);
+    const uint32_t pt = warp_excl_scan(stri, tt);
+    for (uint32_t k = 0; k < R; ++k) {
+        const uint32_t q = lane * R + k;
+        if (q >= BB) break;
+        vp[q] += pv;
+        if (want_tris) tp[q] += pt;
     }
-
-    while (true) {
-        if (threadIdx.x == 0) misc[32] = atomicAdd(ticket, 1u);
-        __syncthreads();
-        const uint32_t r = misc[32];
-        __syncthreads();
-        if (r >= count) break;
-        const uint32_t id = ids[r];
-        const Geo g = block_geo(id, B, p.GX, p.GY, p.X, tma, sizeof(T));
-        bool ok = stage_tile<T>(p, &map, pl, g, smem, bar, phase, tma, st);
-        if (ok) row_masks<T>(p, pl, g, smem);
-        __syncthreads();
-
-        // per-row vertex and triangle counts; thread t owns a contiguous run of rows
-        constexpr int RPT_MAX = 4;  // rows per thread for B <= 16 with NT >= 64
-        const uint32_t rpt = (BB + NT - 1) / NT;
-        uint32_t nv_t = 0, nt_t = 0;
-        uint32_t rv[RPT_MAX], rt[RPT_MAX];
-#pragma unroll
-        for (int k = 0; k < RPT_MAX; ++k) {
-            rv[k] = rt[k] = 0;
-            const uint32_t q = threadIdx.x * rpt + k;
-            if (!ok || (uint32_t)k >= rpt || q >= BB) continue;
-            const uint32_t y = q % B, z = q / B;
-            uint32_t xc, yc, zc;
-            row_cross(p, pl, g, rows, y, z, xc, yc, zc);
-            cross[q] = xc;
-            cross[BB + q] = yc;
-            cross[2 * BB + q] = zc;
-            rv[k] = __popc(xc) + __popc(yc) + __popc(zc);
-            const uint32_t ncell = cells_in_row(p, pl, g, y, z);
-            uint32_t ntr = 0;
-            if (ncell) {
-                const uint32_t r00 = rows[z * pl.B1 + y], r01 = rows[z * pl.B1 + y + 1];
-                const uint32_t r10 = rows[(z + 1) * pl.B1 + y], r11 = rows[(z + 1) * pl.B1 + y + 1];
-                const uint32_t span = (2u << ncell) - 1u;  // bits 0..ncell
-                const uint32_t a = r00 & r01 & r10 & r11 & span, o = (r00 | r01 | r10 | r11) & span;
-                const bool uniform = (a == span) || (o == 0);
-                for (uint32_t x = 0; x < ncell; ++x) {
-                    const uint32_t cfg = uniform ? (a ? 255u : 0u) : cell_case(r00, r01, r10, r11, x);
-                    ntr += ntab[cfg];
-                    if (cell_cases) cell_cases[(uint64_t)r * B * BB + q * B + x] = (uint8_t)cfg;
-                }
-            }
-            if (cell_cases)
-                for (uint32_t x = ncell; x < B; ++x) cell_cases[(uint64_t)r * B * BB + q * B + x] = 0;
-            rt[k] = ntr;
-            nv_t += rv[k];
-            nt_t += ntr;
-        }
-        uint64_t tot64;
-        const uint64_t pre =
-            cta_exclusive_scan64<NT>(((uint64_t)nt_t << 32) | nv_t, reinterpret_cast<uint64_t *>(misc64), &tot64);
-        uint32_t pv = (uint32_t)pre, pt = (uint32_t)(pre >> 32);
-#pragma unroll
-        for (int k = 0; k < RPT_MAX; ++k) {
-            const uint32_t q = threadIdx.x * rpt + k;
-            if ((uint32_t)k < rpt && q < BB) {
-                vp[q] = pv;
-                tp[q] = pt;
-                pv += rv[k];
-                pt += rt[k];
-            }
-        }
-        const uint32_t bnv = (uint32_t)tot64, bnt = (uint32_t)(tot64 >> 32);
-
-        // ---- decoupled look-back over ranks: status = [63:62] flag, [61:31] tris, [30:0] verts
-        if (threadIdx.x < 32) {
-            const uint32_t lane = threadIdx.x;
-            uint64_t sv = 0, stt = 0;
-            bool abort = !ok;
-            const uint64_t agg = ((uint64_t)bnt << 31) | bnv;
-            if (r == 0) {
-                // nothing before
-            } else {
-                if (lane == 0 && !abort) st_volatile(&status[r], (1ull << 62) | agg);
-                int64_t j = (int64_t)r - 1;
-                uint32_t spins = 0;
-                while (!abort) {
-                    const int64_t k = j - (int64_t)lane;
-                    const uint64_t w = k >= 0 ? ld_volatile(&status[k]) : (2ull << 62);
-                    const uint32_t flag = (uint32_t)(w >> 62);
-                    if (__any_sync(0xffffffffu, flag == 3u)) { abort = true; break; }
-                    const uint32_t inc = __ballot_sync(0xffffffffu, flag == 2u);
-                    const uint32_t emp = __ballot_sync(0xffffffffu, flag == 0u);
-                    const uint32_t first = inc ? (uint32_t)(__ffs(inc) - 1) : 32u;
-                    const uint32_t window = first >= 31 ? 0xffffffffu : ((2u << first) - 1u);
-                    if (emp & window) {
-                        if (++spins >= kSpinLimit) {
-                            if (lane == 0) report(st, MTX_ERR_TIMEOUT, kSiteCountLookback, r, (uint32_t)j);
-                            abort = true;
-                            break;
-                        }
-                        backoff(spins);
-                        continue;
-                    }
-                    uint64_t a = lane <= first ? (w & kCnt31) : 0ull;
-                    uint64_t b = lane <= first ? ((w >> 31) & kCnt31) : 0ull;
-#pragma unroll
-                    for (int o = 16; o; o >>= 1) {
-                        a += __shfl_xor_sync(0xffffffffu, a, o);
-                        b += __shfl_xor_sync(0xffffffffu, b, o);
-                    }
-                    sv += a;
-                    stt += b;
-                    if (first < 32) break;
-                    j -= 32;
-                }
-            }
-            const uint64_t iv = sv + bnv, it = stt + bnt;
-            if (!abort && (iv > kCnt31 || it > kCnt31 || 3ull * it > 0xffffffffull)) {
-                if (lane == 0) report(st, MTX_ERR_CAPACITY, kSiteCountOverflow, (uint32_t)(iv >> 32), (uint32_t)it);
-                abort = true;
-            }
-            if (lane == 0) {
-                st_volatile(&status[r], abort ? (3ull << 62) : ((2ull << 62) | (it << 31) | iv));
-                misc[33] = abort ? 1u : 0u;
-                misc64[17] = (stt << 32) | sv;
-            }
-        }
-        __syncthreads();
-        if (!misc[33]) {
-            const uint64_t pre2 = misc64[17];
-            const uint32_t vbase = (uint32_t)pre2, tbase = (uint32_t)(pre2 >> 32);
-            if (threadIdx.x == 0) {
-                if (r < desc_capacity) {
-                    mtx_meshlet_descriptor d;
-                    d.vertexOffset = vbase;
-                    d.indexOffset = 3u * tbase;
-                    d.vertexCount = bnv;
-                    d.primitiveCount = bnt;
-                    desc[r] = d;
-                } else {
-                    report(st, MTX_ERR_CAPACITY, kSiteEmitCapacity, r, 0);
-                }
-                if (r == count - 1) {
-                    totals[0] = vbase + bnv;
-                    totals[1] = 3u * (tbase + bnt);
-                    totals[2] = count;
-                    totals[3] = count;
-                }
-            }
-            // low-face records: prefix | mask << 24 of voxels with x == 0, y == 0, z == 0
-            uint32_t *fr = faces + (uint64_t)r * 3 * BB;
-            for (uint32_t e = threadIdx.x; e < 3 * BB; e += NT) {
-                const uint32_t f = e / BB, i = e % BB;
-                const uint32_t a = i % B, b = i / B;
-                uint32_t x, y, z;
-                if (f == 0) { x = 0; y = a; z = b; }
-                else if (f == 1) { x = a; y = 0; z = b; }
-                else { x = a; y = b; z = 0; }
-                const uint32_t q = z * B + y;
-                const uint32_t below = (1u << x) - 1u;
-                const uint32_t xc = cross[q], yc = cross[BB + q], zc = cross[2 * BB + q];
-                const uint32_t pre = vp[q] + __popc(xc & below) + __popc(yc & below) + __popc(zc & below);
-                const uint32_t m = ((xc >> x) & 1u) | (((yc >> x) & 1u) << 1) | (((zc >> x) & 1u) << 2);
-                fr[e] = pre | (m << 24);
-            }
-        }
-        const bool stop = misc[33] != 0;
-        __syncthreads();
-        if (stop) break;  // successors see the aborted status and stop too
-    }
+    __syncwarp();
+    nv = tv;
+    nt = tt;
 }
 
-// -------------------------------------------------------------- emit pass
-constexpr uint32_t kNoVertex = 0xffffffffu;
-
-template <typename T>
-__device__ __forceinline__ float tile_val(const Plan &pl, const Geo &g, const unsigned char *smem, uint32_t x,
-                                          uint32_t y, uint32_t z) {
-    const T *tile = reinterpret_cast<const T *>(smem + pl.off_tile);
-    return Vox<T>::val(tile[(z * pl.B1 + y) * pl.PX + g.xoff + x]);
+// Owned-edge mask of voxel (x, y, z) of the block, from the crossing rows.
+__device__ __forceinline__ uint32_t voxel_mask(const uint32_t *cross, uint32_t BB, uint32_t q, uint32_t x) {
+    return ((cross[q] >> x) & 1u) | (((cross[BB + q] >> x) & 1u) << 1) | (((cross[2 * BB + q] >> x) & 1u) << 2);
 }
 
+// Block-relative index of the first vertex owned by voxel (x, y, z).
+__device__ __forceinline__ uint32_t voxel_prefix(const uint32_t *cross, const uint32_t *vp, uint32_t BB, uint32_t q,
+                                                 uint32_t x) {
+    const uint32_t below = (1u << x) - 1u;
+    return vp[q] + __popc(cross[q] & below) + __popc(cross[BB + q] & below) + __popc(cross[2 * BB + q] & below);
+}
+
+// ------------------------------------------------------------- numerics
 // Edge parameter (marching_cubes_pmb.mesh.glsl:129-134): t = (iso - a)/(b - a)
 // when |b - a| > 1e-5 else 0.5, clamped to [0, 1]; every operation rounds once.
 __device__ __forceinline__ float edge_t(float fa, float fb, float iso) {
@@ -446,240 +405,556 @@ __device__ __forceinline__ void voxel_normal(const Problem &p, uint32_t x, uint3
     normalize3(n[0], n[1], n[2]);
 }
 
-template <typename T, int NT>
-__global__ void __launch_bounds__(NT) emit_kernel(Problem p, const __grid_constant__ CUtensorMap map, bool tma,
-                                                  const uint32_t *__restrict__ ids,
-                                                  const uint32_t *__restrict__ rank_map,
-                                                  const uint32_t *__restrict__ count_ptr,
-                                                  const mtx_meshlet_descriptor *__restrict__ desc,
-                                                  const uint32_t *__restrict__ faces, void *__restrict__ vertices,
-                                                  uint64_t vcap, uint32_t *__restrict__ indices, uint64_t tcap,
-                                                  uint32_t vfmt, uint32_t frame, uint32_t normals,
-                                                  uint64_t block_cap, DevStatus *st) {
-    extern __shared__ __align__(128) unsigned char smem[];
-    const Plan pl = make_plan(p.B, sizeof(T), tma, true);
-    uint32_t *rows = reinterpret_cast<uint32_t *>(smem + pl.off_rows);
-    uint32_t *cross = reinterpret_cast<uint32_t *>(smem + pl.off_cross);
-    uint32_t *vp = reinterpret_cast<uint32_t *>(smem + pl.off_vp);
-    uint32_t *tp = reinterpret_cast<uint32_t *>(smem + pl.off_tp);
-    uint32_t *vid = reinterpret_cast<uint32_t *>(smem + pl.off_vid);
-    uint8_t *vm = smem + pl.off_vm;
-    uint64_t *tab = reinterpret_cast<uint64_t *>(smem + pl.off_tab);
-    uint32_t *misc = reinterpret_cast<uint32_t *>(smem + pl.off_misc);
-    uint64_t *misc64 = reinterpret_cast<uint64_t *>(smem + pl.off_misc);
-    // misc: [0..15] u64 scan scratch; [40..47] neighbour vbase; [48..55] neighbour rank
-    uint64_t *bar = reinterpret_cast<uint64_t *>(smem + pl.off_misc + 448);
+// Normal of the vertex at parameter t on the +axis edge of volume voxel
+// (gx, gy, gz): normalize(mix(n1, n2, t)) (marching_cubes_pmb.mesh.glsl:126-137).
+template <typename T>
+__device__ __noinline__ float3 vertex_normal(const Problem &p, uint32_t gx, uint32_t gy, uint32_t gz, uint32_t a,
+                                             float t) {
+    float n1[3], n2[3];
+    voxel_normal<T>(p, gx, gy, gz, n1);
+    voxel_normal<T>(p, gx + (a == 0), gy + (a == 1), gz + (a == 2), n2);
+    const float omt = __fsub_rn(1.0f, t);
+    float3 n;
+    n.x = __fadd_rn(__fmul_rn(n1[0], omt), __fmul_rn(n2[0], t));
+    n.y = __fadd_rn(__fmul_rn(n1[1], omt), __fmul_rn(n2[1], t));
+    n.z = __fadd_rn(__fmul_rn(n1[2], omt), __fmul_rn(n2[2], t));
+    normalize3(n.x, n.y, n.z);
+    return n;
+}
 
-    for (uint32_t i = threadIdx.x; i < 256; i += NT) tab[i] = c_mc_cases[i];
-    if (threadIdx.x == 0 && tma) {
+// Position of the vertex on the +axis edge of block voxel (x,y,z); its edge
+// parameter goes to *tout.
+template <typename T>
+__device__ __forceinline__ float3 vertex_pos(const Problem &p, const WPlan &pl, const T *tile, const Geo &g, uint32_t x,
+                                             uint32_t y, uint32_t z, uint32_t a, bool ndc, float *tout) {
+    const uint32_t i0 = (z * pl.B1 + y) * pl.PX + g.xoff + x;
+    const uint32_t i1 = i0 + (a == 0 ? 1u : a == 1 ? pl.PX : pl.PX * pl.B1);
+    const float t = edge_t(Vox<T>::val(tile[i0]), Vox<T>::val(tile[i1]), p.iso);
+    *tout = t;
+    float3 pos = make_float3((float)(g.ox + x), (float)(g.oy + y), (float)(g.oz + z));
+    if (a == 0) pos.x = __fadd_rn(pos.x, t);
+    else if (a == 1) pos.y = __fadd_rn(pos.y, t);
+    else pos.z = __fadd_rn(pos.z, t);
+    if (ndc) {
+        pos.x = __fsub_rn(__fmul_rn(__fdiv_rn(pos.x, (float)p.X), 2.0f), 1.0f);
+        pos.y = __fsub_rn(__fmul_rn(__fdiv_rn(pos.y, (float)p.Y), 2.0f), 1.0f);
+        pos.z = __fsub_rn(__fmul_rn(__fdiv_rn(pos.z, (float)p.Z), 2.0f), 1.0f);
+    }
+    return pos;
+}
+
+
+// Writes the block's own vertices (vbase .. vbase + nv) in canonical order.
+// Each lane walks the cut edges of its rows and writes one job per vertex
+// (voxel index | axis << 12) at the vertex's own position in a window of
+// kJobWin jobs; the warp then resolves the window 32 vertices at a time, one
+// per lane, staging positions in shared memory for coalesced stores.
+// GENERIC selects the VertexData / NDC / normals options; the plain form
+// writes xyz in the voxel frame.
+template <typename T, bool GENERIC>
+__device__ __forceinline__ void emit_vertices(const Problem &p, const WPlan &pl, unsigned char *ws, uint32_t buf,
+                                              const Geo &g, uint32_t vbase, uint32_t nv, void *vertices, uint32_t vfmt,
+                                              uint32_t frame, uint32_t normals) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t B = pl.B, BB = pl.BB, R = (BB + 31) / 32;
+    const uint32_t *cross = reinterpret_cast<const uint32_t *>(ws + pl.off_cross);
+    const uint32_t *vp = reinterpret_cast<const uint32_t *>(ws + pl.off_vp);
+    const T *tile = reinterpret_cast<const T *>(ws + pl.off_tile[buf]);
+    float *stage = reinterpret_cast<float *>(ws + pl.off_stage);
+    uint32_t *jobs = reinterpret_cast<uint32_t *>(ws + pl.off_jobs);
+    const bool xyz = !GENERIC || vfmt == MTX_VERTEX_XYZ;
+    for (uint32_t w0 = 0; w0 < nv; w0 += kJobWin) {
+        const uint32_t w1 = w0 + kJobWin;
+        for (uint32_t k = 0; k < R; ++k) {
+            const uint32_t q = lane * R + k;
+            if (q >= BB) break;
+            const uint32_t xc = cross[q], yc = cross[BB + q], zc = cross[2 * BB + q];
+            uint32_t j = vp[q];
+            if (j >= w1 || j + __popc(xc) + __popc(yc) + __popc(zc) <= w0) continue;
+            uint32_t any = xc | yc | zc;
+            while (any) {
+                const uint32_t x = __ffs(any) - 1;
+                any &= any - 1u;
+                const uint32_t base = (q * B + x);
+                if ((xc >> x) & 1u) { if (j >= w0 && j < w1) jobs[j - w0] = base; ++j; }
+                if ((yc >> x) & 1u) { if (j >= w0 && j < w1) jobs[j - w0] = base | (1u << 12); ++j; }
+                if ((zc >> x) & 1u) { if (j >= w0 && j < w1) jobs[j - w0] = base | (2u << 12); ++j; }
+            }
+        }
+        __syncwarp();
+        const uint32_t cnt = min(kJobWin, nv - w0);
+        for (uint32_t b = 0; b < cnt; b += 32) {
+            const uint32_t n = min(32u, cnt - b);
+            if (lane < n) {
+                const uint32_t job = jobs[b + lane];
+                const uint32_t i = job & 0xfffu, a = job >> 12;
+                const uint32_t q = fdiv(i, pl.rB), x = i - q * B;
+                const uint32_t z = fdiv(q, pl.rB), y = q - z * B;
+                float t;
+                const float3 pos =
+                    vertex_pos<T>(p, pl, tile, g, x, y, z, a, GENERIC && frame == MTX_FRAME_NDC, &t);
+                if (xyz) {
+                    stage[3 * lane + 0] = pos.x;
+                    stage[3 * lane + 1] = pos.y;
+                    stage[3 * lane + 2] = pos.z;
+                } else {
+                    float3 nn = make_float3(0.0f, 0.0f, 0.0f);
+                    if (normals) nn = vertex_normal<T>(p, g.ox + x, g.oy + y, g.oz + z, a, t);
+                    float4 *v = reinterpret_cast<float4 *>(vertices) + 2ull * (vbase + w0 + b + lane);
+                    v[0] = make_float4(pos.x, pos.y, pos.z, 1.0f);
+                    v[1] = make_float4(nn.x, nn.y, nn.z, 0.0f);
+                }
+            }
+            __syncwarp();
+            if (xyz) {
+                float *dst = reinterpret_cast<float *>(vertices) + 3ull * (vbase + w0 + b);
+                for (uint32_t w = lane; w < 3 * n; w += 32) dst[w] = stage[w];
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// ------------------------------------------------------------- count pass
+// Per active block: the vertex and triangle counts (into the descriptor's
+// count fields) and the low-face records -- the block-relative prefix and
+// owned-edge mask of every voxel with x == 0 (index z*B+y), y == 0
+// (BB + z*B+x) and z == 0 (2BB + y*B+x).  Blocks are dealt to warps
+// statically, so each warp can prefetch its next tile.
+template <typename T, bool TMA>
+__global__ void __launch_bounds__(kMaxWarps * 32)
+    pmb_count_kernel(Problem p, const __grid_constant__ CUtensorMap map, const uint32_t *__restrict__ ids,
+                     const uint32_t *__restrict__ count_ptr, mtx_meshlet_descriptor *__restrict__ desc,
+                     uint64_t desc_cap, uint32_t *__restrict__ faces, uint32_t *totals,
+                     uint8_t *__restrict__ cell_cases, uint64_t block_cap, DevStatus *st) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const WPlan pl = make_wplan(p.B, sizeof(T), TMA, false);
+    uint8_t *ntab = smem + 2048;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, W = blockDim.x >> 5;
+    unsigned char *ws = smem + kTableBytes + warp * pl.bytes;
+    for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) ntab[i] = (uint8_t)(c_mc_cases[i] & 0xFu);
+    if (lane == 0 && TMA) {
+        uint64_t *bar = reinterpret_cast<uint64_t *>(ws + pl.off_bar);
         mbar_init(bar, 1);
+        mbar_init(bar + 1, 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    const uint32_t count = *count_ptr;
+    if (count > block_cap || count > desc_cap) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            report(st, MTX_ERR_CAPACITY, kSiteEmitCapacity, count, 3);
+            totals[3] = count;
+        }
+        return;
+    }
+    const uint32_t B = pl.B, BB = pl.BB, B3 = BB * B;
+    const uint32_t *cross = reinterpret_cast<const uint32_t *>(ws + pl.off_cross);
+    const uint32_t *vp = reinterpret_cast<const uint32_t *>(ws + pl.off_vp);
+    const uint32_t gw = blockIdx.x * W + warp, nw = gridDim.x * W;
+    uint32_t parity = 0, buf = 0;
+
+    uint32_t r = gw;
+    Geo g{};
+    if (r < count) {
+        g = block_geo(__ldg(ids + r), p, TMA, sizeof(T));
+        tile_issue<T, TMA>(pl, ws, buf, g, &map);
+    }
+    while (r < count) {
+        const uint32_t rn = r + nw;
+        Geo gn{};
+        const bool have_next = rn < count;
+        if (have_next) {
+            gn = block_geo(__ldg(ids + rn), p, TMA, sizeof(T));
+            if (pl.nbuf == 2) tile_issue<T, TMA>(pl, ws, buf ^ 1u, gn, &map);
+        }
+        if (!tile_wait<T, TMA>(p, pl, ws, buf, g, parity, st)) {
+            if (have_next && pl.nbuf == 2) tile_drain<TMA>(pl, ws, buf ^ 1u, parity);
+            break;
+        }
+        build_rows<T>(p, pl, ws, buf, g);
+        uint32_t bnv, bnt;
+        block_counts(p, pl, ws, g, ntab, true, cell_cases ? cell_cases + (uint64_t)r * B3 : nullptr, bnv, bnt);
+        if (lane == 0) *reinterpret_cast<uint2 *>(&desc[r].vertexCount) = make_uint2(bnv, bnt);
+        uint32_t *fr = faces + (uint64_t)r * 3 * BB;
+        for (uint32_t e = lane; e < 3 * BB; e += 32) {
+            const uint32_t f = fdiv(e, pl.rBB), i = e - f * BB, b = fdiv(i, pl.rB), a = i - b * B;
+            const uint32_t x = f == 0 ? 0 : a, y = f == 0 ? a : (f == 1 ? 0 : b), z = f == 2 ? 0 : b;
+            const uint32_t q = z * B + y;
+            fr[e] = voxel_prefix(cross, vp, BB, q, x) | (voxel_mask(cross, BB, q, x) << 24);
+        }
+        if (!have_next) break;
+        if (pl.nbuf == 1) tile_issue<T, TMA>(pl, ws, buf, gn, &map);
+        else buf ^= 1u;
+        r = rn;
+        g = gn;
+    }
+}
+
+// -------------------------------------------------------------- scan pass
+constexpr uint64_t kCnt31 = 0x7fffffffull;
+
+// Warp-cooperative decoupled look-back over per-tile status words
+// ([63:62] flag 1 aggregate / 2 inclusive / 3 aborted, [61:31] triangles,
+// [30:0] vertices).  Publishes this tile's aggregate, then its inclusive
+// prefix; returns the exclusive prefix, false if aborted.  Totals that do
+// not fit 31 bits (or 3 x triangles that do not fit 32) abort with
+// MTX_ERR_CAPACITY.
+__device__ __forceinline__ bool lookback_counts(uint64_t *status, uint32_t r, uint32_t bnv, uint32_t bnt,
+                                                uint64_t &ev, uint64_t &et, DevStatus *st) {
+    const uint32_t lane = threadIdx.x & 31;
+    ev = et = 0;
+    bool abort = false;
+    if (r > 0) {
+        if (lane == 0) st_volatile(&status[r], (1ull << 62) | ((uint64_t)bnt << 31) | bnv);
+        int64_t j = (int64_t)r - 1;
+        uint32_t spins = 0;
+        while (true) {
+            const int64_t k = j - (int64_t)lane;
+            const uint64_t w = k >= 0 ? ld_volatile(&status[k]) : (2ull << 62);
+            const uint32_t flag = (uint32_t)(w >> 62);
+            if (__any_sync(0xffffffffu, flag == 3u)) {
+                abort = true;
+                break;
+            }
+            const uint32_t inc = __ballot_sync(0xffffffffu, flag == 2u);
+            const uint32_t emp = __ballot_sync(0xffffffffu, flag == 0u);
+            const uint32_t first = inc ? (uint32_t)(__ffs(inc) - 1) : 32u;
+            const uint32_t window = first >= 31 ? 0xffffffffu : ((2u << first) - 1u);
+            if (emp & window) {
+                if (++spins >= kSpinLimit) {
+                    if (lane == 0) report(st, MTX_ERR_TIMEOUT, kSiteCountLookback, r, (uint32_t)j);
+                    abort = true;
+                    break;
+                }
+                backoff(spins);
+                continue;
+            }
+            uint64_t a = lane <= first ? (w & kCnt31) : 0ull;
+            uint64_t b = lane <= first ? ((w >> 31) & kCnt31) : 0ull;
+#pragma unroll
+            for (int o = 16; o; o >>= 1) {
+                a += __shfl_xor_sync(0xffffffffu, a, o);
+                b += __shfl_xor_sync(0xffffffffu, b, o);
+            }
+            ev += a;
+            et += b;
+            if (first < 32) break;
+            j -= 32;
+        }
+    }
+    const uint64_t iv = ev + bnv, it = et + bnt;
+    if (!abort && (iv > kCnt31 || it > kCnt31 || 3ull * it > 0xffffffffull)) {
+        if (lane == 0) report(st, MTX_ERR_CAPACITY, kSiteCountOverflow, (uint32_t)(iv >> 32), (uint32_t)it);
+        abort = true;
+    }
+    if (lane == 0) st_volatile(&status[r], abort ? (3ull << 62) : ((2ull << 62) | (it << 31) | iv));
+    return !abort;
+}
+
+// Exclusive scan of the per-block vertex and triangle counts in rank order:
+// each CTA takes 1024 descriptors by ticket and resolves its offset with a
+// decoupled look-back over the tiles before it, then fills vertexOffset and
+// indexOffset.  The last tile writes the totals.
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__global__ void __launch_bounds__(kScanThreads)
+    pmb_scan_kernel(mtx_meshlet_descriptor *__restrict__ desc, const uint32_t *__restrict__ count_ptr,
+                    uint64_t *tile_status, uint32_t *ticket, uint32_t *totals, DevStatus *st) {
+    __shared__ uint32_t s_tile, s_ok;
+    __shared__ uint64_t s_tmp[kScanThreads / 32 + 1];
+    __shared__ uint64_t s_pre[2];
+    if (threadIdx.x == 0) s_tile = atomicAdd(ticket, 1u);
+    __syncthreads();
+    const uint32_t t = s_tile;
+    const uint32_t count = *count_ptr;
+    const uint32_t ntiles = (count + kScanTile - 1) / kScanTile;
+    if (t >= ntiles) return;
+    const uint32_t base = t * kScanTile + threadIdx.x * kScanItems;
+    uint32_t nv[kScanItems], nt[kScanItems], sv = 0, stt = 0;
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        nv[i] = nt[i] = 0;
+        if (base + i < count) {
+            const uint2 c = *reinterpret_cast<const uint2 *>(&desc[base + i].vertexCount);
+            nv[i] = c.x;
+            nt[i] = c.y;
+        }
+        sv += nv[i];
+        stt += nt[i];
+    }
+    uint64_t tot;
+    const uint64_t pre = cta_exclusive_scan64<kScanThreads>(((uint64_t)stt << 32) | sv, s_tmp, &tot);
+    if (threadIdx.x < 32) {
+        uint64_t ev, et;
+        const bool ok = lookback_counts(tile_status, t, (uint32_t)tot, (uint32_t)(tot >> 32), ev, et, st);
+        if (threadIdx.x == 0) {
+            s_ok = ok;
+            s_pre[0] = ev;
+            s_pre[1] = et;
+            if (ok && t == ntiles - 1) {
+                totals[0] = (uint32_t)(ev + (uint32_t)tot);
+                totals[1] = 3u * (uint32_t)(et + (uint32_t)(tot >> 32));
+                totals[2] = count;
+                totals[3] = count;
+            }
+        }
+    }
+    __syncthreads();
+    if (!s_ok) return;
+    uint32_t v = (uint32_t)s_pre[0] + (uint32_t)pre, tr = (uint32_t)s_pre[1] + (uint32_t)(pre >> 32);
+#pragma unroll
+    for (int i = 0; i < kScanItems; ++i) {
+        if (base + i < count) {
+            *reinterpret_cast<uint2 *>(&desc[base + i].vertexOffset) = make_uint2(v, 3u * tr);
+            v += nv[i];
+            tr += nt[i];
+        }
+    }
+}
+
+// -------------------------------------------------------------- emit pass
+// Index of a voxel of the (B+1)^3 context outside the block (some coordinate == B).
+__device__ __forceinline__ uint32_t ctx_index(uint32_t B, uint32_t x, uint32_t y, uint32_t z) {
+    const uint32_t B1 = B + 1;
+    if (x == B) return z * B1 + y;
+    if (y == B) return B1 * B1 + z * B + x;
+    return B1 * B1 + B * B1 + y * B + x;
+}
+
+// Context voxel of compact index j (inverse of ctx_index).
+__device__ __forceinline__ void ctx_voxel(const WPlan &pl, uint32_t j, uint32_t &x, uint32_t &y, uint32_t &z) {
+    const uint32_t B = pl.B, B1 = pl.B1;
+    if (j < B1 * B1) {
+        x = B;
+        z = fdiv(j, pl.rB1);
+        y = j - z * B1;
+    } else if (j < B1 * B1 + B * B1) {
+        const uint32_t i = j - B1 * B1;
+        y = B;
+        z = fdiv(i, pl.rB);
+        x = i - z * B;
+    } else {
+        const uint32_t i = j - B1 * B1 - B * B1;
+        z = B;
+        y = fdiv(i, pl.rB);
+        x = i - y * B;
+    }
+}
+
+// Resolves the vertex id of edge e of the cell at block cell (x, y, z).
+__device__ __forceinline__ uint32_t edge_vertex(uint32_t x, uint32_t y, uint32_t z, uint32_t e, const uint8_t *owner,
+                                                const uint32_t *cross, const uint32_t *vp, const uint32_t *nvid,
+                                                const uint8_t *nm, uint32_t B, uint32_t BB, uint32_t vbase,
+                                                bool &bad) {
+    const uint32_t own = owner[e];
+    const uint32_t ux = x + (own & 1u), uy = y + ((own >> 1) & 1u), uz = z + ((own >> 2) & 1u);
+    const uint32_t ax = own >> 3;
+    uint32_t base, m;
+    if (ux < B && uy < B && uz < B) {
+        const uint32_t q = uz * B + uy;
+        base = vbase + voxel_prefix(cross, vp, BB, q, ux);
+        m = voxel_mask(cross, BB, q, ux);
+    } else {
+        const uint32_t jx = ctx_index(B, ux, uy, uz);
+        base = nvid[jx];
+        m = nm[jx];
+    }
+    if (base == kNoVertex || !((m >> ax) & 1u)) {
+        bad = true;
+        return 0;
+    }
+    return base + __popc(m & ((1u << ax) - 1u));
+}
+
+// CPL: context voxels per lane, ceil((3B^2 + 3B + 1) / 32): 8 covers B <= 8, 32 covers B <= 16
+template <typename T, int CPL, bool TMA, bool GENERIC>
+__global__ void __launch_bounds__(kMaxWarps * 32)
+    pmb_emit_kernel(Problem p, const __grid_constant__ CUtensorMap map, const uint32_t *__restrict__ ids,
+                    const uint32_t *__restrict__ rank_map, const uint32_t *__restrict__ count_ptr,
+                    const mtx_meshlet_descriptor *__restrict__ desc, const uint32_t *__restrict__ faces,
+                    uint32_t *__restrict__ indices, uint64_t tcap, uint64_t block_cap, void *__restrict__ vertices,
+                    uint64_t vcap, uint32_t vfmt, uint32_t frame, uint32_t normals, DevStatus *st) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const WPlan pl = make_wplan(p.B, sizeof(T), TMA, true);
+    uint64_t *tab = reinterpret_cast<uint64_t *>(smem);
+    uint8_t *ntab = smem + 2048;
+    uint8_t *owner = smem + 2048 + 256;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, W = blockDim.x >> 5;
+    unsigned char *ws = smem + kTableBytes + warp * pl.bytes;
+    for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) {
+        tab[i] = c_mc_cases[i];
+        ntab[i] = (uint8_t)(c_mc_cases[i] & 0xFu);
+    }
+    if (threadIdx.x < 12) owner[threadIdx.x] = c_mc_owner[threadIdx.x];
+    if (lane == 0 && TMA) {
+        uint64_t *bar = reinterpret_cast<uint64_t *>(ws + pl.off_bar);
+        mbar_init(bar, 1);
+        mbar_init(bar + 1, 1);
         fence_mbar_init();
     }
     __syncthreads();
     const uint32_t count = *count_ptr;
     if (count > block_cap) return;  // reported by the count pass
-    const uint32_t B = p.B, BB = B * B, B1 = pl.B1;
-    uint32_t phase = 0;
-    const uint64_t nvert_cap = vcap, ntri_cap = tcap;
+    const uint32_t B = pl.B, BB = pl.BB, B1 = pl.B1;
+    const uint32_t *rows = reinterpret_cast<const uint32_t *>(ws + pl.off_rows);
+    const uint32_t *cross = reinterpret_cast<const uint32_t *>(ws + pl.off_cross);
+    const uint32_t *vp = reinterpret_cast<const uint32_t *>(ws + pl.off_vp);
+    const uint32_t *tp = reinterpret_cast<const uint32_t *>(ws + pl.off_tp);
+    uint32_t *nvid = reinterpret_cast<uint32_t *>(ws + pl.off_nvid);
+    uint8_t *nm = ws + pl.off_nm;
+    uint32_t *stage = reinterpret_cast<uint32_t *>(ws + pl.off_stage);
+    uint32_t *jobs = reinterpret_cast<uint32_t *>(ws + pl.off_jobs);
+    const uint32_t gw = blockIdx.x * W + warp, nw = gridDim.x * W;
+    uint32_t parity = 0, buf = 0;
 
-    for (uint32_t r = blockIdx.x; r < count; r += gridDim.x) {
-        const mtx_meshlet_descriptor d = desc[r];
-        if (d.vertexCount == 0 && d.primitiveCount == 0) continue;
+    // lane c in 1..7 holds the rank of neighbour c = (dx, dy, dz) bits (or kNoVertex)
+    auto neighbour_rank = [&](const Geo &gg, uint32_t id) -> uint32_t {
+        uint32_t rk = kNoVertex;
+        if (lane >= 1 && lane < 8) {
+            const uint32_t dx = lane & 1u, dy = (lane >> 1) & 1u, dz = lane >> 2;
+            if (gg.bx + dx < p.GX && gg.by + dy < p.GY && gg.bz + dz < p.GZ)
+                rk = __ldg(rank_map + id + dx + dy * p.GX + dz * p.GX * p.GY);
+        }
+        return rk;
+    };
+
+    uint32_t r = gw;
+    Geo g{};
+    mtx_meshlet_descriptor d{};
+    uint32_t nb_rk = kNoVertex;
+    if (r < count) {
+        const uint32_t id = __ldg(ids + r);
+        g = block_geo(id, p, TMA, sizeof(T));
+        tile_issue<T, TMA>(pl, ws, buf, g, &map);
+        d = desc[r];
+        nb_rk = neighbour_rank(g, id);
+    }
+    while (r < count) {
+        // prefetch the next block: its tile, descriptor and neighbour ranks
+        const uint32_t rn = r + nw;
+        const bool have_next = rn < count;
+        Geo gn{};
+        mtx_meshlet_descriptor dn{};
+        uint32_t nb_rk_n = kNoVertex;
+        if (have_next) {
+            const uint32_t idn = __ldg(ids + rn);
+            gn = block_geo(idn, p, TMA, sizeof(T));
+            if (pl.nbuf == 2) tile_issue<T, TMA>(pl, ws, buf ^ 1u, gn, &map);
+            dn = desc[rn];
+            nb_rk_n = neighbour_rank(gn, idn);
+        }
+        // neighbours' first vertex ids and the face records of the +x/+y/+z
+        // layer: every load issued before any is used
+        const uint32_t nb_vb = (nb_rk != kNoVertex) ? __ldg(&desc[nb_rk].vertexOffset) : kNoVertex;
+        const uint32_t nb3 = pl.nb3;
+        uint32_t rec[CPL];
+#pragma unroll
+        for (uint32_t k = 0; k < CPL; ++k) {
+            rec[k] = 0;
+            if (k * 32 >= nb3) continue;  // warp-uniform
+            const uint32_t j = k * 32 + lane;
+            uint32_t x, y, z;
+            ctx_voxel(pl, j < nb3 ? j : 0, x, y, z);
+            const uint32_t dx = x == B, dy = y == B, dz = z == B;
+            const uint32_t c = j < nb3 ? (dx | (dy << 1) | (dz << 2)) : 1u;
+            const uint32_t rk = __shfl_sync(0xffffffffu, nb_rk, c);
+            if (j < nb3 && rk != kNoVertex && g.ox + x < p.X && g.oy + y < p.Y && g.oz + z < p.Z) {
+                const uint32_t lx = dx ? 0 : x, ly = dy ? 0 : y, lz = dz ? 0 : z;
+                const uint32_t e = dx ? lz * B + ly : (dy ? BB + lz * B + lx : 2 * BB + ly * B + lx);
+                rec[k] = __ldg(faces + (uint64_t)rk * 3 * BB + e) | 0x80000000u;  // top bit: present
+            }
+        }
+        if (!tile_wait<T, TMA>(p, pl, ws, buf, g, parity, st)) {
+            if (have_next && pl.nbuf == 2) tile_drain<TMA>(pl, ws, buf ^ 1u, parity);
+            break;
+        }
+#pragma unroll
+        for (uint32_t k = 0; k < CPL; ++k) {
+            if (k * 32 >= nb3) continue;
+            const uint32_t j = k * 32 + lane;
+            uint32_t x, y, z;
+            ctx_voxel(pl, j < nb3 ? j : 0, x, y, z);
+            const uint32_t c = j < nb3 ? ((x == B) | ((y == B) << 1) | ((z == B) << 2)) : 1u;
+            const uint32_t vb = __shfl_sync(0xffffffffu, nb_vb, c);
+            if (j < nb3) {
+                const bool present = rec[k] >> 31;
+                nvid[j] = present ? vb + (rec[k] & 0xffffffu) : kNoVertex;
+                nm[j] = present ? (uint8_t)((rec[k] >> 24) & 7u) : (uint8_t)0;
+            }
+        }
         const uint32_t tbase = d.indexOffset / 3u;
-        if ((uint64_t)d.vertexOffset + d.vertexCount > nvert_cap || (uint64_t)tbase + d.primitiveCount > ntri_cap) {
-            if (threadIdx.x == 0) report(st, MTX_ERR_CAPACITY, kSiteEmitCapacity, r, 1);
-            continue;
-        }
-        const uint32_t id = ids[r];
-        const Geo g = block_geo(id, B, p.GX, p.GY, p.X, tma, sizeof(T));
-        if (threadIdx.x < 7) {
-            // neighbour (dx,dy,dz) = bits of threadIdx.x + 1
-            const uint32_t c = threadIdx.x + 1, dx = c & 1u, dy = (c >> 1) & 1u, dz = c >> 2;
-            uint32_t vb = kNoVertex, rk = kNoVertex;
-            if (g.bx + dx < p.GX && g.by + dy < p.GY && g.bz + dz < p.GZ) {
-                const uint32_t nid = id + dx + dy * p.GX + dz * p.GX * p.GY;
-                const uint32_t cand = rank_map[nid];
-                if (cand < count && ids[cand] == nid) {
-                    rk = cand;
-                    vb = desc[cand].vertexOffset;
-                }
-            }
-            misc[40 + c] = vb;
-            misc[48 + c] = rk;
-        }
-        if (!stage_tile<T>(p, &map, pl, g, smem, bar, phase, tma, st)) return;
-        row_masks<T>(p, pl, g, smem);
-        __syncthreads();
-
-        constexpr int RPT_MAX = 4;
-        const uint32_t rpt = (BB + NT - 1) / NT;
-        uint32_t nv_t = 0, nt_t = 0;
-        uint32_t rv[RPT_MAX], rt[RPT_MAX];
-#pragma unroll
-        for (int k = 0; k < RPT_MAX; ++k) {
-            rv[k] = rt[k] = 0;
-            const uint32_t q = threadIdx.x * rpt + k;
-            if ((uint32_t)k >= rpt || q >= BB) continue;
-            const uint32_t y = q % B, z = q / B;
-            uint32_t xc, yc, zc;
-            row_cross(p, pl, g, rows, y, z, xc, yc, zc);
-            cross[q] = xc;
-            cross[BB + q] = yc;
-            cross[2 * BB + q] = zc;
-            rv[k] = __popc(xc) + __popc(yc) + __popc(zc);
-            const uint32_t ncell = cells_in_row(p, pl, g, y, z);
-            uint32_t ntr = 0;
-            if (ncell) {
-                const uint32_t r00 = rows[z * B1 + y], r01 = rows[z * B1 + y + 1];
-                const uint32_t r10 = rows[(z + 1) * B1 + y], r11 = rows[(z + 1) * B1 + y + 1];
-                const uint32_t span = (2u << ncell) - 1u;
-                const uint32_t a = r00 & r01 & r10 & r11 & span, o = (r00 | r01 | r10 | r11) & span;
-                if (a != span && o != 0)
-                    for (uint32_t x = 0; x < ncell; ++x) ntr += (uint32_t)(tab[cell_case(r00, r01, r10, r11, x)] & 0xFu);
-            }
-            rt[k] = ntr;
-            nv_t += rv[k];
-            nt_t += ntr;
-        }
-        uint64_t tot64;
-        const uint64_t pre = cta_exclusive_scan64<NT>(((uint64_t)nt_t << 32) | nv_t, misc64, &tot64);
-        uint32_t pv = (uint32_t)pre, pt = (uint32_t)(pre >> 32);
-#pragma unroll
-        for (int k = 0; k < RPT_MAX; ++k) {
-            const uint32_t q = threadIdx.x * rpt + k;
-            if ((uint32_t)k < rpt && q < BB) {
-                vp[q] = pv;
-                tp[q] = pt;
-                pv += rv[k];
-                pt += rt[k];
-            }
-        }
-        if (threadIdx.x == 0 && ((uint32_t)tot64 != d.vertexCount || (uint32_t)(tot64 >> 32) != d.primitiveCount))
-            report(st, MTX_ERR_INTERNAL, kSiteEmitNeighbour, r, 2);
-        __syncthreads();
-
-        // first-vertex id and owned-edge mask of every voxel of the (B+1)^3 context
-        const uint32_t nctx = B1 * B1 * B1;
-        for (uint32_t i = threadIdx.x; i < nctx; i += NT) {
-            const uint32_t x = i % B1, y = (i / B1) % B1, z = i / (B1 * B1);
-            uint32_t first = kNoVertex, mask = 0;
-            if (x < B && y < B && z < B) {
-                const uint32_t q = z * B + y, below = (1u << x) - 1u;
-                const uint32_t xc = cross[q], yc = cross[BB + q], zc = cross[2 * BB + q];
-                first = d.vertexOffset + vp[q] + __popc(xc & below) + __popc(yc & below) + __popc(zc & below);
-                mask = ((xc >> x) & 1u) | (((yc >> x) & 1u) << 1) | (((zc >> x) & 1u) << 2);
-            } else if (g.ox + x < p.X && g.oy + y < p.Y && g.oz + z < p.Z) {
-                const uint32_t dx = x == B, dy = y == B, dz = z == B;
-                const uint32_t c = dx | (dy << 1) | (dz << 2);
-                const uint32_t rk = misc[48 + c];
-                if (rk != kNoVertex) {
-                    const uint32_t lx = dx ? 0 : x, ly = dy ? 0 : y, lz = dz ? 0 : z;
-                    uint32_t e;
-                    if (dx) e = lz * B + ly;
-                    else if (dy) e = BB + lz * B + lx;
-                    else e = 2 * BB + ly * B + lx;
-                    const uint32_t rec = __ldg(faces + (uint64_t)rk * 3 * BB + e);
-                    first = misc[40 + c] + (rec & 0xffffffu);
-                    mask = rec >> 24;
-                }
-            }
-            vid[i] = first;
-            vm[i] = (uint8_t)mask;
-        }
-        __syncthreads();
-
-        // vertices: one thread per owned voxel row
-        for (uint32_t q = threadIdx.x; q < BB; q += NT) {
-            const uint32_t y = q % B, z = q / B;
-            const uint32_t xc = cross[q], yc = cross[BB + q], zc = cross[2 * BB + q];
-            uint32_t any = xc | yc | zc;
-            uint32_t idx = d.vertexOffset + vp[q];
-            while (any) {
-                const uint32_t x = __ffs(any) - 1;
-                any &= any - 1;
-                const uint32_t m = ((xc >> x) & 1u) | (((yc >> x) & 1u) << 1) | (((zc >> x) & 1u) << 2);
-                const float fa = tile_val<T>(pl, g, smem, x, y, z);
-#pragma unroll
-                for (uint32_t a = 0; a < 3; ++a) {
-                    if (!((m >> a) & 1u)) continue;
-                    const float fb = tile_val<T>(pl, g, smem, x + (a == 0), y + (a == 1), z + (a == 2));
-                    const float t = edge_t(fa, fb, p.iso);
-                    float pos[3] = {(float)(g.ox + x), (float)(g.oy + y), (float)(g.oz + z)};
-                    pos[a] = __fadd_rn(pos[a], t);
-                    if (frame == MTX_FRAME_NDC) {
-                        const float dims[3] = {(float)p.X, (float)p.Y, (float)p.Z};
-#pragma unroll
-                        for (int k = 0; k < 3; ++k)
-                            pos[k] = __fsub_rn(__fmul_rn(__fdiv_rn(pos[k], dims[k]), 2.0f), 1.0f);
+        if ((uint64_t)tbase + d.primitiveCount > tcap ||
+            (vertices && (uint64_t)d.vertexOffset + d.vertexCount > vcap)) {
+            if (lane == 0) report(st, MTX_ERR_CAPACITY, kSiteEmitCapacity, r, 2);
+        } else if (d.primitiveCount || (vertices && d.vertexCount)) {
+            build_rows<T>(p, pl, ws, buf, g);
+            uint32_t bnv, bnt;
+            block_counts(p, pl, ws, g, ntab, true, nullptr, bnv, bnt);
+            if (lane == 0 && (bnv != d.vertexCount || bnt != d.primitiveCount))
+                report(st, MTX_ERR_INTERNAL, kSiteEmitNeighbour, r, 2);
+            if (vertices && bnv)
+                emit_vertices<T, GENERIC>(p, pl, ws, buf, g, d.vertexOffset, bnv, vertices, vfmt, frame, normals);
+            // triangles in canonical order: each lane walks the mixed cells of
+            // its rows and writes one job per triangle (cell | t << 12 |
+            // case << 16) at the triangle's own position in a window of
+            // kJobWin jobs; the warp resolves 32 triangles at a time
+            const uint32_t R = (BB + 31) / 32, nt = d.primitiveCount;
+            bool bad = false;
+            for (uint32_t w0 = 0; w0 < nt; w0 += kJobWin) {
+                const uint32_t w1 = w0 + kJobWin;
+                for (uint32_t k = 0; k < R; ++k) {
+                    const uint32_t q = lane * R + k;
+                    if (q >= BB) break;
+                    uint32_t j = tp[q];
+                    const uint32_t jend = (q + 1 < BB) ? tp[q + 1] : nt;
+                    if (j >= w1 || jend <= w0) continue;
+                    const uint32_t z = fdiv(q, pl.rB), y = q - z * B;
+                    uint32_t inside;
+                    uint32_t mm = mixed_cells(p, pl, g, rows, y, z, inside);
+                    while (mm) {
+                        const uint32_t x = __ffs(mm) - 1;
+                        mm &= mm - 1u;
+                        const uint32_t cfg = cell_case(rows, B1, x, y, z);
+                        const uint32_t n = ntab[cfg];
+                        for (uint32_t t = 0; t < n; ++t, ++j)
+                            if (j >= w0 && j < w1) jobs[j - w0] = (q * B + x) | (t << 12) | (cfg << 16);
                     }
-                    if (vfmt == MTX_VERTEX_XYZ) {
-                        float *v = reinterpret_cast<float *>(vertices) + 3ull * idx;
-                        v[0] = pos[0];
-                        v[1] = pos[1];
-                        v[2] = pos[2];
-                    } else {
-                        float nrm[3] = {0.f, 0.f, 0.f};
-                        if (normals) {
-                            float n1[3], n2[3];
-                            const uint32_t gx = g.ox + x, gy = g.oy + y, gz = g.oz + z;
-                            voxel_normal<T>(p, gx, gy, gz, n1);
-                            voxel_normal<T>(p, gx + (a == 0), gy + (a == 1), gz + (a == 2), n2);
-                            const float omt = __fsub_rn(1.0f, t);
-#pragma unroll
-                            for (int k = 0; k < 3; ++k) nrm[k] = __fadd_rn(__fmul_rn(n1[k], omt), __fmul_rn(n2[k], t));
-                            normalize3(nrm[0], nrm[1], nrm[2]);
-                        }
-                        float4 *v = reinterpret_cast<float4 *>(vertices) + 2ull * idx;
-                        v[0] = make_float4(pos[0], pos[1], pos[2], 1.0f);
-                        v[1] = make_float4(nrm[0], nrm[1], nrm[2], 0.0f);
+                }
+                __syncwarp();
+                const uint32_t cnt = min(kJobWin, nt - w0);
+                for (uint32_t b = 0; b < cnt; b += 32) {
+                    const uint32_t n = min(32u, cnt - b);
+                    if (lane < n) {
+                        const uint32_t job = jobs[b + lane];
+                        const uint32_t i = job & 0xfffu, t = (job >> 12) & 7u;
+                        const uint32_t q = fdiv(i, pl.rB), x = i - q * B;
+                        const uint32_t z = fdiv(q, pl.rB), y = q - z * B;
+                        const uint64_t w = tab[job >> 16] >> (4 + 12 * t);
+                        stage[3 * lane + 0] = edge_vertex(x, y, z, (uint32_t)(w & 0xFu), owner, cross, vp, nvid, nm,
+                                                          B, BB, d.vertexOffset, bad);
+                        stage[3 * lane + 1] = edge_vertex(x, y, z, (uint32_t)((w >> 4) & 0xFu), owner, cross, vp,
+                                                          nvid, nm, B, BB, d.vertexOffset, bad);
+                        stage[3 * lane + 2] = edge_vertex(x, y, z, (uint32_t)((w >> 8) & 0xFu), owner, cross, vp,
+                                                          nvid, nm, B, BB, d.vertexOffset, bad);
                     }
-                    ++idx;
+                    __syncwarp();
+                    uint32_t *dst = indices + 3ull * (tbase + w0 + b);
+                    for (uint32_t q = lane; q < 3 * n; q += 32) dst[q] = stage[q];
+                    __syncwarp();
                 }
             }
+            if (bad) report(st, MTX_ERR_INTERNAL, kSiteEmitNeighbour, r, 3);
         }
-
-        // triangles: one thread per cell row
-        for (uint32_t q = threadIdx.x; q < BB; q += NT) {
-            const uint32_t y = q % B, z = q / B;
-            const uint32_t ncell = cells_in_row(p, pl, g, y, z);
-            if (!ncell) continue;
-            const uint32_t r00 = rows[z * B1 + y], r01 = rows[z * B1 + y + 1];
-            const uint32_t r10 = rows[(z + 1) * B1 + y], r11 = rows[(z + 1) * B1 + y + 1];
-            const uint32_t span = (2u << ncell) - 1u;
-            const uint32_t a = r00 & r01 & r10 & r11 & span, o = (r00 | r01 | r10 | r11) & span;
-            if (a == span || o == 0) continue;
-            uint64_t tri = (uint64_t)tbase + tp[q];
-            for (uint32_t x = 0; x < ncell; ++x) {
-                const uint32_t cfg = cell_case(r00, r01, r10, r11, x);
-                const uint64_t w = tab[cfg];
-                const uint32_t n = (uint32_t)(w & 0xFu);
-                for (uint32_t t = 0; t < n; ++t, ++tri) {
-                    uint32_t out[3];
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) {
-                        const uint32_t e = (uint32_t)((w >> (4 + 4 * (3 * t + k))) & 0xFu);
-                        const uint32_t own = c_mc_owner[e];
-                        const uint32_t ux = x + (own & 1u), uy = y + ((own >> 1) & 1u), uz = z + ((own >> 2) & 1u);
-                        const uint32_t ax = own >> 3;
-                        const uint32_t li = (uz * B1 + uy) * B1 + ux;
-                        const uint32_t msk = vm[li];
-                        uint32_t v = vid[li];
-                        if (v == kNoVertex || !((msk >> ax) & 1u)) {
-                            report(st, MTX_ERR_INTERNAL, kSiteEmitNeighbour, r, li);
-                            v = 0;
-                        } else {
-                            v += __popc(msk & ((1u << ax) - 1u));
-                        }
-                        out[k] = v;
-                    }
-                    uint32_t *dst = indices + 3ull * tri;
-                    dst[0] = out[0];
-                    dst[1] = out[1];
-                    dst[2] = out[2];
-                }
-            }
-        }
-        __syncthreads();
+        if (!have_next) break;
+        if (pl.nbuf == 1) tile_issue<T, TMA>(pl, ws, buf, gn, &map);
+        else buf ^= 1u;
+        r = rn;
+        d = dn;
+        g = gn;
+        nb_rk = nb_rk_n;
     }
 }
 
@@ -704,60 +979,59 @@ static bool use_tma(const Problem &p, uint32_t staging) {
     return tma_ok(p);
 }
 
-template <typename T, int NT>
-static mtx_status run_count(mtx_context *c, const Problem &p, const ExtractArgs &a, const CUtensorMap &map, bool tma,
-                            cudaStream_t s) {
-    const Plan pl = make_plan(p.B, sizeof(T), tma, false);
-    auto k = count_kernel<T, NT>;
-    MTX_CUDA(c, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.bytes));
+template <typename K>
+static mtx_status grid_for(mtx_context *c, K kernel, int threads, uint32_t smem, uint32_t host_count, int warps,
+                           unsigned &grid) {
+    MTX_CUDA(c, cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    MTX_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NT, pl.bytes));
-    uint64_t grid = (uint64_t)std::max(per_sm, 1) * c->sm_count;
-    if (a.host_count) grid = std::min<uint64_t>(grid, a.host_count);
-    grid = std::max<uint64_t>(grid, 1);
-    k<<<(unsigned)grid, NT, pl.bytes, s>>>(p, map, tma, a.ids, a.count, a.desc, a.desc_capacity, a.faces,
-                                          a.count_status, &c->ctrl->count_ticket, a.totals, a.cell_cases,
-                                          a.block_capacity, &c->ctrl->status);
+    MTX_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
+    if (per_sm < 1) return fail(c, MTX_ERR_UNSUPPORTED, "extraction kernel does not fit on an SM");
+    uint64_t g = (uint64_t)per_sm * c->sm_count;
+    if (host_count) g = std::min<uint64_t>(g, (host_count + warps - 1) / warps);
+    grid = (unsigned)std::max<uint64_t>(g, 1);
+    return MTX_OK;
+}
+
+template <typename T>
+static mtx_status run_count(mtx_context *c, const Problem &p, const ExtractArgs &a, const CUtensorMap &map, bool tma,
+                            uint32_t W, cudaStream_t s) {
+    const WPlan pl = make_wplan(p.B, sizeof(T), tma, false);
+    const uint32_t smem = kTableBytes + W * pl.bytes;
+    auto k = tma ? pmb_count_kernel<T, true> : pmb_count_kernel<T, false>;
+    unsigned grid;
+    mtx_status r = grid_for(c, k, W * 32, smem, a.host_count, W, grid);
+    if (r != MTX_OK) return r;
+    k<<<grid, W * 32, smem, s>>>(p, map, a.ids, a.count, a.desc, a.desc_capacity, a.faces, a.totals, a.cell_cases,
+                                 a.block_capacity, &c->ctrl->status);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "count launch");
     return MTX_OK;
 }
 
-template <typename T, int NT>
+template <typename T, int CPL, bool TMA>
+static void (*emit_fn(bool generic))(Problem, CUtensorMap, const uint32_t *, const uint32_t *, const uint32_t *,
+                                     const mtx_meshlet_descriptor *, const uint32_t *, uint32_t *, uint64_t, uint64_t,
+                                     void *, uint64_t, uint32_t, uint32_t, uint32_t, DevStatus *) {
+    return generic ? pmb_emit_kernel<T, CPL, TMA, true> : pmb_emit_kernel<T, CPL, TMA, false>;
+}
+
+template <typename T>
 static mtx_status run_emit(mtx_context *c, const Problem &p, const ExtractArgs &a, const CUtensorMap &map, bool tma,
-                           cudaStream_t s) {
-    const Plan pl = make_plan(p.B, sizeof(T), tma, true);
-    auto k = emit_kernel<T, NT>;
-    MTX_CUDA(c, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)pl.bytes));
-    int per_sm = 0;
-    MTX_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, NT, pl.bytes));
-    uint64_t grid = (uint64_t)std::max(per_sm, 1) * c->sm_count;
-    if (a.host_count) grid = std::min<uint64_t>(grid, a.host_count);
-    grid = std::max<uint64_t>(grid, 1);
-    k<<<(unsigned)grid, NT, pl.bytes, s>>>(p, map, tma, a.ids, a.rank_map, a.count, a.desc, a.faces, a.vertices,
-                                          a.vertex_capacity, a.indices, a.tri_capacity, a.vertex_format, a.frame,
-                                          a.normals, a.block_capacity, &c->ctrl->status);
+                           uint32_t W, cudaStream_t s) {
+    const WPlan pl = make_wplan(p.B, sizeof(T), tma, true);
+    const uint32_t smem = kTableBytes + W * pl.bytes;
+    const bool generic = a.vertices && (a.vertex_format != MTX_VERTEX_XYZ || a.frame != MTX_FRAME_VOXEL);
+    auto k = p.B <= 8 ? (tma ? emit_fn<T, 8, true>(generic) : emit_fn<T, 8, false>(generic))
+                      : (tma ? emit_fn<T, 32, true>(generic) : emit_fn<T, 32, false>(generic));
+    unsigned grid;
+    mtx_status r = grid_for(c, k, W * 32, smem, a.host_count, W, grid);
+    if (r != MTX_OK) return r;
+    k<<<grid, W * 32, smem, s>>>(p, map, a.ids, a.rank_map, a.count, a.desc, a.faces, a.indices, a.tri_capacity,
+                                 a.block_capacity, a.vertices, a.vertex_capacity, a.vertex_format, a.frame, a.normals,
+                                 &c->ctrl->status);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "emit launch");
     return MTX_OK;
-}
-
-static int pick_threads(uint32_t B, uint32_t req) {
-    if (req == 64 || req == 128 || req == 256) {
-        // rows per thread must stay <= 4
-        if ((B * B + req - 1) / req <= 4) return (int)req;
-    }
-    return B * B <= 64 ? 64 : (B * B <= 128 ? 128 : 256);
-}
-
-template <int NT, bool EMIT>
-static mtx_status dispatch_nt(mtx_context *c, const Problem &p, const ExtractArgs &a, const CUtensorMap &map, bool tma,
-                              cudaStream_t s) {
-    switch (p.dtype) {
-    case MTX_DTYPE_U8: return EMIT ? run_emit<uint8_t, NT>(c, p, a, map, tma, s) : run_count<uint8_t, NT>(c, p, a, map, tma, s);
-    case MTX_DTYPE_U16: return EMIT ? run_emit<uint16_t, NT>(c, p, a, map, tma, s) : run_count<uint16_t, NT>(c, p, a, map, tma, s);
-    default: return EMIT ? run_emit<float, NT>(c, p, a, map, tma, s) : run_count<float, NT>(c, p, a, map, tma, s);
-    }
 }
 
 template <bool EMIT>
@@ -765,28 +1039,42 @@ static mtx_status launch_stage(mtx_context *c, const Problem &p, const ExtractAr
     if (p.B < 2 || p.B > MTX_MAX_BLOCK_EDGE) return fail(c, MTX_ERR_UNSUPPORTED, "block edge must be in [2, 16]");
     mtx_status rs = ensure_tables(c);
     if (rs != MTX_OK) return rs;
-    const bool tma = use_tma(p, a.staging);
+    const uint32_t staging = a.staging ? a.staging : c->tuning.staging;
+    const bool tma = use_tma(p, staging);
     CUtensorMap map;
     memset(&map, 0, sizeof(map));
     if (tma) {
-        const Plan pl = make_plan(p.B, dtype_size(p.dtype), true, EMIT);
-        rs = make_volume_tensor_map(c, p, pl.PX, &map);
+        rs = make_volume_tensor_map(c, p, tile_pitch(p.B, dtype_size(p.dtype), true), &map);
         if (rs != MTX_OK) return rs;
     }
-    switch (pick_threads(p.B, a.threads)) {
-    case 64: return dispatch_nt<64, EMIT>(c, p, a, map, tma, s);
-    case 128: return dispatch_nt<128, EMIT>(c, p, a, map, tma, s);
-    default: return dispatch_nt<256, EMIT>(c, p, a, map, tma, s);
+    // warps per CTA: threads/32 of the options, else the context's tuning, else 4
+    uint32_t W = a.threads ? a.threads / 32 : (c->tuning.extractWarps ? c->tuning.extractWarps : 4);
+    W = std::min<uint32_t>(std::max<uint32_t>(W, 1), kMaxWarps);
+    switch (p.dtype) {
+    case MTX_DTYPE_U8: return EMIT ? run_emit<uint8_t>(c, p, a, map, tma, W, s) : run_count<uint8_t>(c, p, a, map, tma, W, s);
+    case MTX_DTYPE_U16: return EMIT ? run_emit<uint16_t>(c, p, a, map, tma, W, s) : run_count<uint16_t>(c, p, a, map, tma, W, s);
+    default: return EMIT ? run_emit<float>(c, p, a, map, tma, W, s) : run_count<float>(c, p, a, map, tma, W, s);
     }
 }
 
+// Counts, faces and the scan: after this the descriptors and totals are final.
 mtx_status launch_count(mtx_context *c, const Problem &p, const ExtractArgs &a, cudaStream_t s) {
+    const uint64_t cap = std::min<uint64_t>(a.block_capacity, a.desc_capacity);
+    const uint32_t ntiles = (uint32_t)std::max<uint64_t>(1, (cap + kScanTile - 1) / kScanTile);
+    mtx_status r = scratch_reserve(c, c->count_status, sizeof(uint64_t) * (size_t)ntiles);
+    if (r != MTX_OK) return r;
     MTX_CUDA(c, cudaMemsetAsync(&c->ctrl->count_ticket, 0, sizeof(uint32_t), s));
     MTX_CUDA(c, cudaMemsetAsync(a.totals, 0, 4 * sizeof(uint32_t), s));
-    if (a.host_count) MTX_CUDA(c, cudaMemsetAsync(a.count_status, 0, sizeof(uint64_t) * a.host_count, s));
-    return launch_stage<false>(c, p, a, s);
+    MTX_CUDA(c, cudaMemsetAsync(c->count_status.ptr, 0, sizeof(uint64_t) * ntiles, s));
+    if ((r = launch_stage<false>(c, p, a, s)) != MTX_OK) return r;
+    pmb_scan_kernel<<<ntiles, kScanThreads, 0, s>>>(a.desc, a.count, (uint64_t *)c->count_status.ptr,
+                                                    &c->ctrl->count_ticket, a.totals, &c->ctrl->status);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(c, e, "scan launch");
+    return MTX_OK;
 }
 
+// Vertices (when a.vertices is set) and triangles.
 mtx_status launch_emit(mtx_context *c, const Problem &p, const ExtractArgs &a, cudaStream_t s) {
     return launch_stage<true>(c, p, a, s);
 }

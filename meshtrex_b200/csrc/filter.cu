@@ -7,7 +7,9 @@
 // each CTA takes a tile of 1024 consecutive block ids by ticket, counts its
 // active blocks (warp scan + CTA scan), and resolves its global offset with a
 // single-pass decoupled look-back over the tiles before it: the list comes out
-// in ascending block order, which is the order the CPU rule produces.
+// in ascending block order, which is the order the CPU rule produces.  It
+// also writes the rank of every block (0xffffffff for inactive ones), which
+// the extraction uses to find a neighbouring block's vertices.
 #include "mtx_internal.h"
 
 namespace mtx {
@@ -103,15 +105,25 @@ __global__ void __launch_bounds__(kFilterThreads)
     __syncthreads();
     if (s_abort) return;
     uint32_t r = s_prefix + excl;
+    // rank of every block of the tile: its rank if active, else kNoRank
+    uint32_t rk[kFilterItems];
 #pragma unroll
     for (int i = 0; i < kFilterItems; ++i) {
+        rk[i] = 0xffffffffu;
         if (f[i]) {
             const uint32_t id = (uint32_t)(base + i);
             ids[r] = id;
-            rank_map[id] = r;
+            rk[i] = r;
             if (count_status) count_status[r] = 0ull;
             ++r;
         }
+    }
+    if (base + kFilterItems <= nblocks) {
+        *reinterpret_cast<uint4 *>(rank_map + base) = make_uint4(rk[0], rk[1], rk[2], rk[3]);
+    } else {
+#pragma unroll
+        for (int i = 0; i < kFilterItems; ++i)
+            if (base + i < nblocks) rank_map[base + i] = rk[i];
     }
     if (t == ntiles - 1 && threadIdx.x == 0) *count_out = s_prefix + total;
 }

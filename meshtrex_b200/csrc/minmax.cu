@@ -64,7 +64,7 @@ template <> struct Lane16<float> {
     }
 };
 
-template <typename T, int B>
+template <typename T, int B, int ZU>
 __global__ void __launch_bounds__(128) minmax_leaf_vec_kernel(const T *__restrict__ vol, uint32_t X,
                                                               uint32_t Y, uint32_t Z, uint32_t GX,
                                                               uint32_t GY, uint32_t GZ, uint32_t nXS,
@@ -75,6 +75,7 @@ __global__ void __launch_bounds__(128) minmax_leaf_vec_kernel(const T *__restric
     constexpr int SEG = 32 * V;
     constexpr int NB = V >= B ? V / B : 1;      // blocks per lane
     constexpr int LPB = V >= B ? 1 : B / V;     // lanes per block
+    constexpr int CNT = V >= B ? B : V;         // elements of one block in one lane
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t w = (uint64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (w >= nwarps) return;  // uniform per warp
@@ -100,79 +101,87 @@ __global__ void __launch_bounds__(128) minmax_leaf_vec_kernel(const T *__restric
 
     const uint32_t zend = min(bz1 * B, Z - 1);
     uint32_t bz = bz0;
-    for (uint32_t z = bz0 * B; z <= zend; ++z) {
-        const T *row = vol + (uint64_t)z * plane + (uint64_t)y0 * X;
-        uint4 mn = L16::lo_id(), mx = L16::hi_id();
-        uint32_t hmn = ~0u, hmx = 0u;
-        if (on) {
+    for (uint32_t z0 = bz0 * B; z0 <= zend; z0 += ZU) {
+        // issue every load of the ZU slices before any of them is folded
+        uint4 v[ZU][B + 1];
+        uint32_t hv[ZU][B + 1];
+#pragma unroll
+        for (int u = 0; u < ZU; ++u) {
+            const T *row = vol + (uint64_t)(z0 + u) * plane + (uint64_t)y0 * X;
+            const bool zon = z0 + u <= zend;
+#pragma unroll
+            for (int r = 0; r <= B; ++r) {
+                v[u][r] = L16::lo_id();
+                if (on && zon && (uint32_t)r < ny)
+                    v[u][r] = __ldg(reinterpret_cast<const uint4 *>(row + (uint64_t)r * X + x0));
+                hv[u][r] = 0;
+                if (halo_on && zon && (uint32_t)r < ny) hv[u][r] = Vox<T>::key(__ldg(row + (uint64_t)r * X + xh));
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < ZU; ++u) {
+            const uint32_t z = z0 + u;
+            if (z > zend) break;
+            uint4 mn = L16::lo_id(), mx = L16::hi_id();
+            uint32_t hmn = ~0u, hmx = 0u;
 #pragma unroll
             for (int r = 0; r <= B; ++r) {
                 if ((uint32_t)r < ny) {
-                    uint4 v = __ldg(reinterpret_cast<const uint4 *>(row + (uint64_t)r * X + x0));
-                    L16::fold(mn, mx, v);
+                    if (on) L16::fold(mn, mx, v[u][r]);
+                    if (halo_on) {
+                        hmn = min(hmn, hv[u][r]);
+                        hmx = max(hmx, hv[u][r]);
+                    }
                 }
             }
-        }
-        if (halo_on) {
-#pragma unroll
-            for (int r = 0; r <= B; ++r) {
-                if ((uint32_t)r < ny) {
-                    uint32_t k = Vox<T>::key(__ldg(row + (uint64_t)r * X + xh));
-                    hmn = min(hmn, k);
-                    hmx = max(hmx, k);
-                }
-            }
-        }
-        // first column of the next lane is this lane's halo column
-        uint32_t nmn = __shfl_down_sync(0xffffffffu, L16::elem(mn, 0, false), 1);
-        uint32_t nmx = __shfl_down_sync(0xffffffffu, L16::elem(mx, 0, true), 1);
-        if (lane == 31) { nmn = hmn; nmx = hmx; }
+            // first column of the next lane is this lane's halo column
+            uint32_t nmn = __shfl_down_sync(0xffffffffu, L16::elem(mn, 0, false), 1);
+            uint32_t nmx = __shfl_down_sync(0xffffffffu, L16::elem(mx, 0, true), 1);
+            if (lane == 31) { nmn = hmn; nmx = hmx; }
 
-        uint32_t smn[NB], smx[NB];
-#pragma unroll
-        for (int j = 0; j < NB; ++j) {
-            uint32_t a = ~0u, b = 0u;
-            constexpr int CNT = V >= B ? B : V;
-#pragma unroll
-            for (int i = 0; i < CNT; ++i) {
-                a = min(a, L16::elem(mn, j * CNT + i, false));
-                b = max(b, L16::elem(mx, j * CNT + i, true));
-            }
-            const bool take_halo = V >= B ? true : ((lane % LPB) == LPB - 1);
-            if (take_halo) {
-                if (V >= B && j + 1 < NB) {
-                    a = min(a, L16::elem(mn, (j + 1) * B, false));
-                    b = max(b, L16::elem(mx, (j + 1) * B, true));
-                } else {
-                    a = min(a, nmn);
-                    b = max(b, nmx);
-                }
-            }
-            smn[j] = a;
-            smx[j] = b;
-        }
-
-        const bool boundary = z == bz * B + B;  // halo slice of bz, first slice of bz + 1
-#pragma unroll
-        for (int j = 0; j < NB; ++j) { amn[j] = min(amn[j], smn[j]); amx[j] = max(amx[j], smx[j]); }
-        if (boundary) {
-            // write block bz
+            uint32_t smn[NB], smx[NB];
 #pragma unroll
             for (int j = 0; j < NB; ++j) {
-                uint32_t a = amn[j], b = amx[j];
+                uint32_t a = ~0u, b = 0u;
 #pragma unroll
-                for (int o = 1; o < LPB; o <<= 1) {
-                    a = min(a, __shfl_xor_sync(0xffffffffu, a, o));
-                    b = max(b, __shfl_xor_sync(0xffffffffu, b, o));
+                for (int i = 0; i < CNT; ++i) {
+                    a = min(a, L16::elem(mn, j * CNT + i, false));
+                    b = max(b, L16::elem(mx, j * CNT + i, true));
                 }
-                if (on && (lane % LPB) == 0) {
-                    uint32_t bx = x0 / B + j;
-                    leaf[((uint64_t)bz * GY + by) * GX + bx] = make_uint2(a, b);
+                const bool take_halo = V >= B ? true : ((lane % LPB) == LPB - 1);
+                if (take_halo) {
+                    if (V >= B && j + 1 < NB) {
+                        a = min(a, L16::elem(mn, (j + 1) * B, false));
+                        b = max(b, L16::elem(mx, (j + 1) * B, true));
+                    } else {
+                        a = min(a, nmn);
+                        b = max(b, nmx);
+                    }
                 }
-                amn[j] = smn[j];
-                amx[j] = smx[j];
+                smn[j] = a;
+                smx[j] = b;
             }
-            ++bz;
+#pragma unroll
+            for (int j = 0; j < NB; ++j) { amn[j] = min(amn[j], smn[j]); amx[j] = max(amx[j], smx[j]); }
+            if (z == bz * B + B) {
+                // halo slice of bz, first slice of bz + 1: write block bz
+#pragma unroll
+                for (int j = 0; j < NB; ++j) {
+                    uint32_t a = amn[j], b = amx[j];
+#pragma unroll
+                    for (int o = 1; o < LPB; o <<= 1) {
+                        a = min(a, __shfl_xor_sync(0xffffffffu, a, o));
+                        b = max(b, __shfl_xor_sync(0xffffffffu, b, o));
+                    }
+                    if (on && (lane % LPB) == 0) {
+                        const uint32_t bx = x0 / B + j;
+                        leaf[((uint64_t)bz * GY + by) * GX + bx] = make_uint2(a, b);
+                    }
+                    amn[j] = smn[j];
+                    amx[j] = smx[j];
+                }
+                ++bz;
+            }
         }
     }
     if (bz < bz1) {
@@ -185,7 +194,7 @@ __global__ void __launch_bounds__(128) minmax_leaf_vec_kernel(const T *__restric
                 b = max(b, __shfl_xor_sync(0xffffffffu, b, o));
             }
             if (on && (lane % LPB) == 0) {
-                uint32_t bx = x0 / B + j;
+                const uint32_t bx = x0 / B + j;
                 leaf[((uint64_t)bz * GY + by) * GX + bx] = make_uint2(a, b);
             }
         }
@@ -263,7 +272,7 @@ __global__ void __launch_bounds__(512) pyramid3_kernel(PyrLevels L, uint32_t til
 }
 
 // ------------------------------------------------------------------ host
-template <typename T, int B>
+template <typename T, int B, int ZU>
 static cudaError_t launch_vec(const Problem &p, uint2 *leaf, cudaStream_t s, int sm_count, uint32_t zover) {
     constexpr uint32_t SEG = 32 * (16 / sizeof(T));
     uint32_t nXS = ceil_div(p.X, SEG);
@@ -275,8 +284,8 @@ static cudaError_t launch_vec(const Problem &p, uint2 *leaf, cudaStream_t s, int
     nzc = ceil_div(p.GZ, zchunk);
     uint64_t nwarps = cols * nzc;
     uint64_t blocks = (nwarps + 3) / 4;
-    minmax_leaf_vec_kernel<T, B><<<(unsigned)blocks, 128, 0, s>>>((const T *)p.vol, p.X, p.Y, p.Z, p.GX, p.GY,
-                                                                 p.GZ, nXS, zchunk, nwarps, leaf);
+    minmax_leaf_vec_kernel<T, B, ZU><<<(unsigned)blocks, 128, 0, s>>>((const T *)p.vol, p.X, p.Y, p.Z, p.GX, p.GY,
+                                                                     p.GZ, nXS, zchunk, nwarps, leaf);
     return cudaGetLastError();
 }
 
@@ -288,26 +297,36 @@ static cudaError_t launch_generic(const Problem &p, uint2 *leaf, cudaStream_t s)
     return cudaGetLastError();
 }
 
-template <typename T>
-static cudaError_t dispatch_leaf(const Problem &p, uint2 *leaf, cudaStream_t s, int sm, uint32_t zover) {
-    const bool vec_ok = ((uintptr_t)p.vol % 16 == 0) && (((uint64_t)p.X * sizeof(T)) % 16 == 0);
-    if (vec_ok) {
-        switch (p.B) {
-        case 4: return launch_vec<T, 4>(p, leaf, s, sm, zover);
-        case 8: return launch_vec<T, 8>(p, leaf, s, sm, zover);
-        case 16: return launch_vec<T, 16>(p, leaf, s, sm, zover);
-        default: break;
-        }
+template <typename T, int ZU>
+static cudaError_t dispatch_b(const Problem &p, uint2 *leaf, cudaStream_t s, int sm, uint32_t zover) {
+    switch (p.B) {
+    case 4: return launch_vec<T, 4, ZU>(p, leaf, s, sm, zover);
+    case 8: return launch_vec<T, 8, ZU>(p, leaf, s, sm, zover);
+    default: return launch_vec<T, 16, ZU>(p, leaf, s, sm, zover);
     }
-    return launch_generic<T>(p, leaf, s);
+}
+
+template <typename T>
+static cudaError_t dispatch_leaf(const Problem &p, uint2 *leaf, cudaStream_t s, int sm, uint32_t zover,
+                                 uint32_t slices) {
+    const bool vec_ok = ((uintptr_t)p.vol % 16 == 0) && (((uint64_t)p.X * sizeof(T)) % 16 == 0) &&
+                        (p.B == 4 || p.B == 8 || p.B == 16);
+    if (!vec_ok) return launch_generic<T>(p, leaf, s);
+    switch (slices) {
+    case 1: return dispatch_b<T, 1>(p, leaf, s, sm, zover);
+    case 4: return dispatch_b<T, 4>(p, leaf, s, sm, zover);
+    default: return dispatch_b<T, 2>(p, leaf, s, sm, zover);
+    }
 }
 
 mtx_status launch_minmax_leaf(mtx_context *c, const Problem &p, uint2 *leaf, cudaStream_t s, uint32_t zover) {
     cudaError_t e;
+    if (!zover) zover = c->tuning.minmaxZChunk;
+    const uint32_t sl = c->tuning.minmaxSlices;
     switch (p.dtype) {
-    case MTX_DTYPE_U8: e = dispatch_leaf<uint8_t>(p, leaf, s, c->sm_count, zover); break;
-    case MTX_DTYPE_U16: e = dispatch_leaf<uint16_t>(p, leaf, s, c->sm_count, zover); break;
-    default: e = dispatch_leaf<float>(p, leaf, s, c->sm_count, zover); break;
+    case MTX_DTYPE_U8: e = dispatch_leaf<uint8_t>(p, leaf, s, c->sm_count, zover, sl); break;
+    case MTX_DTYPE_U16: e = dispatch_leaf<uint16_t>(p, leaf, s, c->sm_count, zover, sl); break;
+    default: e = dispatch_leaf<float>(p, leaf, s, c->sm_count, zover, sl); break;
     }
     if (e != cudaSuccess) return cuda_fail(c, e, "minmax leaf launch");
     return MTX_OK;

@@ -44,6 +44,7 @@ struct mtx_context {
     uint32_t *pinned = nullptr;  // pinned host words for count readbacks
     mtx::Scratch filter_status, count_status, faces, leaf, ids, rank, desc, misc;
     mtx_profiler *prof = nullptr;  // records stage times of calls given no profiler
+    mtx_tuning tuning = {0, 0, 0, 0};
 };
 
 namespace mtx {
@@ -93,13 +94,15 @@ mtx_status launch_pyramid(mtx_context *c, uint2 *all_levels, int levels, const u
                           const uint64_t *offset, cudaStream_t s);
 
 // Stage 2: ordered compaction of active blocks.
-//   ids[rank] = block id, rank_map[id] = rank, *count = number of active blocks.
-//   count_status (optional): zeroed for every rank, for the count scan.
+//   ids[rank] = block id, rank_map[id] = rank (0xffffffff if inactive),
+//   *count = number of active blocks.  count_status: optional per-rank words
+//   to zero (pass null).
 mtx_status launch_filter(mtx_context *c, const Problem &p, const uint2 *leaf, uint32_t *ids,
                          uint32_t *rank_map, uint32_t *count, uint64_t *count_status, cudaStream_t s);
 
-// Stage 3: per-active-block counts, their scan, face tables and meshlet
-// descriptors; then the emit pass.
+// Stage 3: per-active-block counts and face records, the scan that fills the
+// meshlet descriptors and totals (launch_count); then vertices and triangles
+// (launch_emit).
 struct ExtractArgs {
     const uint32_t *ids;
     const uint32_t *rank_map;
@@ -109,10 +112,10 @@ struct ExtractArgs {
     uint64_t desc_capacity;
     uint32_t *faces;            // 3*B*B words per active block
     uint64_t block_capacity;    // active blocks that desc/faces/count_status can hold
-    uint64_t *count_status;     // look-back words, one per active block, zeroed
+    uint64_t *count_status;     // unused (the scan keeps its own look-back words)
     uint32_t *totals;           // device uint32[4] {vertexCount, indexCount, meshletCount, activeCount}
     uint8_t *cell_cases;        // optional
-    void *vertices;
+    void *vertices;             // vertex buffer written by the emit pass, or null
     uint64_t vertex_capacity;
     uint32_t *indices;
     uint64_t tri_capacity;

@@ -88,3 +88,136 @@ def test_plain_path_matches_oracle(ctx, oracle, shape, dtype, block, staging):
     x.free()
     f.free()
     mm.free()
+
+
+def _mesh_via_async(ctx, vol, block, iso, vcap, tcap, **kw):
+    from meshtrex_b200 import api
+    ex = api.AsyncExtractor(ctx, vol, block, iso, vcap, tcap, **kw)
+    ex.run()
+    ctx.synchronize()
+    c = u32(ex.counters)
+    V, T = int(c[0]), int(c[1]) // 3
+    return ex.vertices[:V].cpu().numpy(), u32(ex.indices[:T]), c
+
+
+@pytest.mark.parametrize("shape,dtype,block", [((40, 36, 48), np.uint8, 8), ((33, 40, 32), np.uint16, 4),
+                                               ((48, 48, 48), np.float32, 16), ((30, 27, 26), np.uint16, 5)])
+def test_async_whole_path_matches_oracle(ctx, oracle, shape, dtype, block):
+    a = blob_volume(shape, dtype, seed=7)
+    iso = mid_iso(a)
+    ref = oracle.extract(a, block, iso)
+    xyz, idx, c = _mesh_via_async(ctx, to_cuda(a), block, iso, ref.n_vertices + 7, ref.n_triangles + 3)
+    assert c[4] == 0 and c[2] == len(ref.ids) and c[3] == len(ref.ids)
+    np.testing.assert_array_equal(xyz.view(np.uint32), ref.xyz.view(np.uint32))
+    np.testing.assert_array_equal(idx, ref.indices)
+
+
+@pytest.mark.parametrize("slices", [1, 2, 4])
+@pytest.mark.parametrize("warps", [1, 2, 8])
+def test_tuning_variants_match_oracle(ctx, oracle, slices, warps):
+    from meshtrex_b200 import api
+    a = blob_volume((36, 40, 64), np.uint16, seed=11)
+    iso = mid_iso(a)
+    ref = oracle.extract(a, 8, iso)
+    ctx.set_tuning(minmax_slices=slices, extract_warps=warps, minmax_zchunk=1 + slices % 3)
+    try:
+        m = api.extract(to_cuda(a), 8, iso, ctx=ctx)
+        np.testing.assert_array_equal(u32(m.leaf).reshape(-1, 2), oracle.minmax_halo(a, 8))
+        np.testing.assert_array_equal(m.vertices.cpu().numpy().view(np.uint32), ref.xyz.view(np.uint32))
+        np.testing.assert_array_equal(u32(m.indices), ref.indices)
+        xyz, idx, c = _mesh_via_async(ctx, to_cuda(a), 8, iso, ref.n_vertices, ref.n_triangles)
+        np.testing.assert_array_equal(xyz.view(np.uint32), ref.xyz.view(np.uint32))
+        np.testing.assert_array_equal(idx, ref.indices)
+    finally:
+        ctx.set_tuning()
+
+
+@pytest.mark.parametrize("dtype", [np.uint8, np.float32])
+def test_vertexdata_normals_and_ndc(ctx, oracle, dtype):
+    from meshtrex_b200 import _lib as L
+    from meshtrex_b200 import api
+    a = blob_volume((34, 30, 32), dtype, seed=5)
+    iso = mid_iso(a)
+    ref = oracle.extract(a, 8, iso, frame=oracle.FRAME_NDC, want_normals=True)
+    opts = api.extract_options(vertex_format=L.VERTEX_DATA, frame=L.FRAME_NDC, normals=True)
+    m = api.extract(to_cuda(a), 8, iso, ctx=ctx, options=opts)
+    v = m.vertices.cpu().numpy()
+    assert v.shape == (ref.n_vertices, 8)
+    np.testing.assert_array_equal(v[:, :3].view(np.uint32), ref.xyz.view(np.uint32))
+    np.testing.assert_array_equal(v[:, 4:7].view(np.uint32), ref.normals.view(np.uint32))
+    assert (v[:, 3] == 1.0).all() and (v[:, 7] == 0.0).all()
+    # the same record written by the count pass (async path)
+    xyz, idx, c = _mesh_via_async(ctx, to_cuda(a), 8, iso, ref.n_vertices, ref.n_triangles, options=opts)
+    np.testing.assert_array_equal(xyz[:, 4:7].view(np.uint32), ref.normals.view(np.uint32))
+    np.testing.assert_array_equal(idx, ref.indices)
+
+
+def test_capacity_overflow_is_reported(ctx, oracle):
+    from meshtrex_b200 import _lib as L
+    from meshtrex_b200 import api
+    a = blob_volume((40, 40, 48), np.uint8, seed=3)
+    iso = mid_iso(a)
+    ref = oracle.extract(a, 8, iso)
+    ex = api.AsyncExtractor(ctx, to_cuda(a), 8, iso, ref.n_vertices // 2, ref.n_triangles // 2)
+    ex.run()
+    with pytest.raises(L.MtxError) as e:
+        ctx.synchronize()
+    assert e.value.status == 4  # MTX_ERR_CAPACITY
+    c = u32(ex.counters)
+    assert c[0] == ref.n_vertices and c[1] == 3 * ref.n_triangles and c[4] == 4
+    ctx.synchronize()  # the error word was cleared
+    # a bound on active blocks that is too small is reported the same way
+    ex = api.AsyncExtractor(ctx, to_cuda(a), 8, iso, ref.n_vertices, ref.n_triangles,
+                            max_active_blocks=max(1, len(ref.ids) // 2))
+    ex.run()
+    with pytest.raises(L.MtxError):
+        ctx.synchronize()
+    assert u32(ex.counters)[3] == len(ref.ids)
+    ctx.synchronize()
+
+
+def test_injected_allocation_failure(oracle):
+    from meshtrex_b200 import _lib as L
+    from meshtrex_b200 import api
+    a = blob_volume((24, 24, 32), np.uint8, seed=1)
+    c = api.Context(0)
+    try:
+        pc = api.push_constants((32, 24, 24), 8, 120.0)
+        v = api.wrap_volume(to_cuda(a))
+        c.fail_allocation(1)
+        with pytest.raises(L.MtxError) as e:
+            api.compute_min_max_mip(c, v, pc)
+        assert e.value.status == 3  # MTX_ERR_OOM
+        mm = api.compute_min_max_mip(c, v, pc)  # the next call allocates normally
+        mm.free()
+    finally:
+        c.close()
+
+
+def test_profiler_stage_names(ctx):
+    from meshtrex_b200 import api
+    a = blob_volume((32, 32, 32), np.uint8, seed=2)
+    prof = api.Profiler(ctx)
+    prof.begin_frame()
+    api.extract(to_cuda(a), 8, 128.5, ctx=ctx, profiler=prof)
+    prof.end_frame()
+    r = prof.regions()
+    for name in ("MinMax_Leaf_Pass", "MinMax_Octree_Reduction", "Active_Block_Filtering", "Mesh_Extraction"):
+        assert name in r and r[name][0] > 0.0
+    prof.close()
+
+
+def test_invalid_arguments_are_rejected(ctx):
+    from meshtrex_b200 import _lib as L
+    from meshtrex_b200 import api
+    a = blob_volume((16, 16, 16), np.uint8, seed=2)
+    v = api.wrap_volume(to_cuda(a))
+    pc = api.push_constants((16, 16, 16), 8, 100.0)
+    pc.blockGridDim[0] = 3
+    with pytest.raises(L.MtxError) as e:
+        api.compute_min_max_mip(ctx, v, pc)
+    assert e.value.status == 1
+    pc = api.push_constants((16, 16, 16), 32, 100.0)
+    with pytest.raises(L.MtxError) as e:
+        api.compute_min_max_mip(ctx, v, pc)
+    assert e.value.status == 2
