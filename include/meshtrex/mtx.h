@@ -238,6 +238,30 @@ mtx_status mtx_filter_active_blocks(mtx_context_t ctx, const mtx_minmax_output *
 mtx_status mtx_read_active_block_count(mtx_context_t ctx, mtx_filtering_output *filt);
 mtx_status mtx_filtering_free(mtx_context_t ctx, mtx_filtering_output *filt);
 
+/* Active-block filtering and ordered compaction that allocates no memory.
+ * No counterpart in meshtrex: it is for callers that cannot allocate device
+ * memory while they run -- an application that owns a fixed device-memory
+ * budget, or code running where cudaMalloc is not allowed -- and that also
+ * cannot hold an mtx context (creating one allocates).  It runs the same
+ * compaction as mtx_filter_active_blocks on the current device and the given
+ * stream, with its scratch in a fixed 256 KiB array inside the library
+ * (every GPU that loads the library keeps it until the process exits), and
+ * calls no allocator.
+ *   leaf_minmax   device, {min,max} keys of total_blocks blocks (mip level 0)
+ *   compacted_ids device, total_blocks words: the active block ids, ascending
+ *   block_rank    device, total_blocks words: rank of each block, 0xffffffff if inactive
+ *   active_count  device, one word
+ *   device_status device, 4 words (optional): {mtx_status, site, info, info}
+ *                 of an error a kernel met, zero otherwise
+ * Limit: total_blocks <= 67,108,864 (65,536 tiles of 1024 blocks), else
+ * MTX_ERR_CAPACITY before any work.  The first call on a device looks up the
+ * array's device address; make that first call before any stream capture.
+ * Every call reuses the same array, so calls that overlap on the GPU race:
+ * issue them one after the other. */
+mtx_status mtx_filter_active_blocks_noalloc(const uint32_t *leaf_minmax, uint64_t total_blocks, uint32_t dtype,
+                                            float isovalue, uint32_t *compacted_ids, uint32_t *block_rank,
+                                            uint32_t *active_count, uint32_t *device_status, void *stream);
+
 /* ------------------------------------------------------------ stage 3 */
 
 /* extractMeshletDescriptors (src/extractionManager.h:10-11,

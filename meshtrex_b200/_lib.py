@@ -113,6 +113,7 @@ SIGNATURES = [
                                        C.POINTER(FilteringOutput)]),
     ("mtx_read_active_block_count", _ST, [_P, C.POINTER(FilteringOutput)]),
     ("mtx_filtering_free", _ST, [_P, C.POINTER(FilteringOutput)]),
+    ("mtx_filter_active_blocks_noalloc", _ST, [_P, C.c_uint64, C.c_uint32, C.c_float, _P, _P, _P, _P, _P]),
     ("mtx_extract_meshlet_descriptors", _ST, [_P, C.POINTER(MinMaxOutput),
                                               C.POINTER(FilteringOutput),
                                               C.POINTER(PushConstants), C.POINTER(ExtractOptions),

@@ -10,6 +10,8 @@
 // in ascending block order, which is the order the CPU rule produces.  It
 // also writes the rank of every block (0xffffffff for inactive ones), which
 // the extraction uses to find a neighbouring block's vertices.
+#include <mutex>
+
 #include "mtx_internal.h"
 
 namespace mtx {
@@ -146,3 +148,84 @@ mtx_status launch_filter(mtx_context *c, const Problem &p, const uint2 *leaf, ui
 }
 
 }  // namespace mtx
+
+// ------------------------------------------------- compaction without allocation
+// Some callers cannot allocate device memory while they run: an application
+// with its own fixed device-memory budget, or code that runs where
+// cudaMalloc is not allowed.  For them, mtx_filter_active_blocks_noalloc
+// runs the same compaction kernel with its scratch (one look-back word per
+// 1024-block tile and a ticket counter) in the statically sized array below
+// instead of a context's arena.  The array lives in every GPU that loads the
+// library until the process exits; it bounds the problem to
+// kNoallocMaxTiles * 1024 blocks.  Calls that overlap on the GPU (two
+// streams, two host threads) share the array and race: serialise them.
+namespace mtx {
+constexpr uint32_t kNoallocMaxTiles = 65536;                // up to 65536 * 1024 = 67,108,864 blocks
+constexpr uint32_t kNoallocTicket = kNoallocMaxTiles;       // word index of the tile ticket
+constexpr uint32_t kNoallocStatus = kNoallocMaxTiles + 4;   // 4 words: error record if the caller passes none
+constexpr uint32_t kNoallocWords = kNoallocMaxTiles + 8;    // 256 KiB + 32 bytes
+}  // namespace mtx
+
+// Words [0, ntiles) hold the look-back status of each tile, then the ticket
+// counter and a fallback error record.
+static __device__ __align__(256) uint32_t g_noalloc_scratch[mtx::kNoallocWords];
+
+namespace {
+// Device address of g_noalloc_scratch, looked up once per device (with that
+// device current).  Host code must not use the symbol itself as a pointer:
+// on the host it names a stand-in object, not device memory.
+uint32_t *g_noalloc_ptr[128] = {nullptr};
+std::mutex g_noalloc_mu;
+
+cudaError_t noalloc_scratch(int device, uint32_t **out) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (device < 0 || device >= 128) return cudaErrorInvalidDevice;
+    if (!g_noalloc_ptr[device]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_noalloc_ptr[device] = static_cast<uint32_t *>(p);
+    }
+    *out = g_noalloc_ptr[device];
+    return cudaSuccess;
+}
+}  // namespace
+
+extern "C" mtx_status mtx_filter_active_blocks_noalloc(const uint32_t *leaf_minmax, uint64_t total_blocks,
+                                                       uint32_t dtype, float isovalue, uint32_t *compacted_ids,
+                                                       uint32_t *block_rank, uint32_t *active_count,
+                                                       uint32_t *device_status, void *stream) {
+    using namespace mtx;
+    if (!leaf_minmax || !compacted_ids || !block_rank || !active_count || dtype > MTX_DTYPE_F32 || total_blocks == 0)
+        return MTX_ERR_INVALID_ARG;
+    if (total_blocks > (uint64_t)kNoallocMaxTiles * kFilterTile) return MTX_ERR_CAPACITY;
+    const uint32_t ntiles = (uint32_t)((total_blocks + kFilterTile - 1) / kFilterTile);
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) {
+        cudaGetLastError();
+        return MTX_ERR_NO_DEVICE;
+    }
+    uint32_t *sc = nullptr;
+    if (noalloc_scratch(device, &sc) != cudaSuccess) {
+        cudaGetLastError();
+        return MTX_ERR_CUDA;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    DevStatus *st = reinterpret_cast<DevStatus *>(device_status ? device_status : sc + kNoallocStatus);
+    // the array keeps the previous call's contents: clear what must start at zero
+    if (cudaMemsetAsync(sc, 0, sizeof(uint32_t) * (size_t)ntiles, s) != cudaSuccess ||
+        cudaMemsetAsync(sc + kNoallocTicket, 0, sizeof(uint32_t), s) != cudaSuccess ||
+        cudaMemsetAsync(active_count, 0, sizeof(uint32_t), s) != cudaSuccess) {
+        cudaGetLastError();
+        return MTX_ERR_CUDA;
+    }
+    if (device_status && cudaMemsetAsync(device_status, 0, sizeof(DevStatus), s) != cudaSuccess) {
+        cudaGetLastError();
+        return MTX_ERR_CUDA;
+    }
+    filter_compact_kernel<<<ntiles, kFilterThreads, 0, s>>>(reinterpret_cast<const uint2 *>(leaf_minmax), total_blocks,
+                                                           ntiles, dtype, isovalue, compacted_ids, block_rank,
+                                                           active_count, nullptr, sc, sc + kNoallocTicket, st);
+    if (cudaGetLastError() != cudaSuccess) return MTX_ERR_CUDA;
+    return MTX_OK;
+}
