@@ -284,6 +284,81 @@ mtx_status mtx_extract_plain_async(mtx_context_t ctx, const mtx_volume *vol,
                                    const mtx_push_constants *pc, const mtx_extract_options *opts,
                                    const mtx_mesh_buffers *out);
 
+/* ------------------------------------------------------------ batches */
+
+/* Many extractions in one go: any number of device-resident volumes (mixed
+ * dtypes and sizes), each extracted at one or more isovalues.  A run is two
+ * launches -- the leaf min/max of every volume, then one persistent kernel
+ * that filters, compacts, counts, scans and emits every job -- and is
+ * recorded once into a CUDA graph when useGraph is set.  meshtrex has no
+ * batched path; each job's output equals what the plain sequence
+ * (mtx_compute_min_max_mip, mtx_filter_active_blocks,
+ * mtx_extract_meshlet_descriptors) gives for that volume, block edge and
+ * isovalue, with the vertex and meshlet offsets counted from the job's own
+ * first vertex and index. */
+typedef struct mtx_batch *mtx_batch_t;
+
+typedef struct mtx_batch_job {
+    uint32_t volume; /* index into mtx_batch_desc::volumes */
+    float isovalue;
+} mtx_batch_job;
+
+typedef struct mtx_batch_desc {
+    uint32_t volumeCount;
+    uint32_t jobCount;
+    const mtx_volume *volumes;   /* device-resident; they must outlive the batch */
+    const uint32_t *blockEdges;  /* per volume, 2..16 */
+    const mtx_batch_job *jobs;
+    /* Pooled capacities over all jobs (0 = a default: every block of every
+     * job; 4 * B^2 vertices and 8 * B^2 triangles per active block, B the
+     * largest block edge).  A run that needs more reports MTX_ERR_CAPACITY
+     * with the sizes it needed in mtx_batch_totals. */
+    uint64_t maxActiveBlocks;
+    uint64_t vertexCapacity;
+    uint64_t triangleCapacity;
+    uint32_t vertexFormat; /* mtx_vertex_format */
+    uint32_t frame;        /* mtx_frame */
+    uint32_t normals;      /* MTX_VERTEX_DATA only */
+    uint32_t useGraph;     /* 1 = record the run into a CUDA graph at the first mtx_batch_run */
+} mtx_batch_desc;
+
+/* One job's slice of the pooled outputs. */
+typedef struct mtx_batch_job_result {
+    uint32_t meshletOffset; /* first meshlet descriptor of the job (= its first active block) */
+    uint32_t meshletCount;  /* active blocks */
+    uint32_t vertexCount;
+    uint32_t indexCount;
+    uint64_t vertexOffset;  /* first vertex of the job in the pooled vertex buffer */
+    uint64_t indexOffset;   /* first index of the job in the pooled index buffer */
+} mtx_batch_job_result;
+
+/* Totals of a run.  On MTX_ERR_CAPACITY they are the sizes the run needed. */
+typedef struct mtx_batch_totals {
+    int32_t status; /* mtx_status of the run */
+    uint32_t activeBlocks;
+    uint64_t vertexCount;
+    uint64_t triangleCount;
+} mtx_batch_totals;
+
+typedef struct mtx_batch_outputs {
+    mtx_buffer vertexBuffer;            /* pooled vertices of every job */
+    mtx_buffer indexBuffer;             /* uint32; each job's indices count from its own first vertex */
+    mtx_buffer meshletDescriptorBuffer; /* pooled; offsets count from the job's first vertex and index */
+    mtx_buffer jobResultBuffer;         /* mtx_batch_job_result[jobCount] */
+    uint32_t vertexStride;              /* 12 or 32 bytes */
+    uint32_t _pad;
+} mtx_batch_outputs;
+
+/* Allocates everything a run needs (no allocation happens in mtx_batch_run). */
+mtx_status mtx_batch_create(mtx_context_t ctx, const mtx_batch_desc *desc, mtx_batch_t *out);
+/* Enqueues one run on the context's stream; does not wait. */
+mtx_status mtx_batch_run(mtx_batch_t b);
+mtx_status mtx_batch_get_outputs(mtx_batch_t b, mtx_batch_outputs *out);
+/* Waits for the last run, then copies the per-job results (results may be
+ * NULL; else jobCount entries) and the totals (may be NULL). */
+mtx_status mtx_batch_read_results(mtx_batch_t b, mtx_batch_job_result *results, mtx_batch_totals *totals);
+mtx_status mtx_batch_destroy(mtx_batch_t b);
+
 /* ------------------------------------------------------------ profiler */
 
 /* GPUProfiler (src/gpuProfiler.h:11-160): CUDA events around the stage

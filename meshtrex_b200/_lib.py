@@ -88,6 +88,35 @@ class MeshBuffers(C.Structure):
                 ("counters", C.c_void_p), ("maxActiveBlocks", C.c_uint64)]
 
 
+class BatchJob(C.Structure):
+    _fields_ = [("volume", C.c_uint32), ("isovalue", C.c_float)]
+
+
+class BatchDesc(C.Structure):
+    _fields_ = [("volumeCount", C.c_uint32), ("jobCount", C.c_uint32),
+                ("volumes", C.POINTER(Volume)), ("blockEdges", C.POINTER(C.c_uint32)),
+                ("jobs", C.POINTER(BatchJob)), ("maxActiveBlocks", C.c_uint64),
+                ("vertexCapacity", C.c_uint64), ("triangleCapacity", C.c_uint64),
+                ("vertexFormat", C.c_uint32), ("frame", C.c_uint32), ("normals", C.c_uint32),
+                ("useGraph", C.c_uint32)]
+
+
+class BatchJobResult(C.Structure):
+    _fields_ = [("meshletOffset", C.c_uint32), ("meshletCount", C.c_uint32),
+                ("vertexCount", C.c_uint32), ("indexCount", C.c_uint32),
+                ("vertexOffset", C.c_uint64), ("indexOffset", C.c_uint64)]
+
+
+class BatchTotals(C.Structure):
+    _fields_ = [("status", C.c_int32), ("activeBlocks", C.c_uint32),
+                ("vertexCount", C.c_uint64), ("triangleCount", C.c_uint64)]
+
+
+class BatchOutputs(C.Structure):
+    _fields_ = [("vertexBuffer", Buffer), ("indexBuffer", Buffer), ("meshletDescriptorBuffer", Buffer),
+                ("jobResultBuffer", Buffer), ("vertexStride", C.c_uint32), ("_pad", C.c_uint32)]
+
+
 # (name, restype, argtypes) of every exported entry point
 _P = C.c_void_p
 _ST = C.c_int
@@ -121,6 +150,11 @@ SIGNATURES = [
     ("mtx_extraction_free", _ST, [_P, C.POINTER(ExtractionOutput)]),
     ("mtx_extract_plain_async", _ST, [_P, C.POINTER(Volume), C.POINTER(PushConstants),
                                       C.POINTER(ExtractOptions), C.POINTER(MeshBuffers)]),
+    ("mtx_batch_create", _ST, [_P, C.POINTER(BatchDesc), C.POINTER(_P)]),
+    ("mtx_batch_run", _ST, [_P]),
+    ("mtx_batch_get_outputs", _ST, [_P, C.POINTER(BatchOutputs)]),
+    ("mtx_batch_read_results", _ST, [_P, _P, C.POINTER(BatchTotals)]),
+    ("mtx_batch_destroy", _ST, [_P]),
     ("mtx_profiler_create", _ST, [_P, C.POINTER(_P)]),
     ("mtx_context_set_profiler", _ST, [_P, _P]),
     ("mtx_context_set_tuning", _ST, [_P, C.POINTER(Tuning)]),

@@ -357,3 +357,75 @@ class AsyncExtractor:
         L.check(L.lib().mtx_extract_plain_async(self.ctx.handle, C.byref(self.vol), C.byref(self.pc),
                                                 C.byref(self.opts), C.byref(self.bufs)),
                 "mtx_extract_plain_async", self.ctx.handle)
+
+
+class Batch:
+    """Many (volume, isovalue) jobs in one run (mtx_batch_*): a batched min/max
+    launch and one persistent extraction kernel, recorded into a CUDA graph when
+    use_graph is set.  volumes are CUDA tensors [z, y, x] of any supported
+    dtype; blocks gives each volume's block edge; jobs is a list of
+    (volume index, isovalue)."""
+
+    def __init__(self, ctx: Context, volumes, blocks, jobs, max_active_blocks: int = 0,
+                 vertex_capacity: int = 0, triangle_capacity: int = 0,
+                 options: L.ExtractOptions | None = None, use_graph: bool = True):
+        self.ctx = ctx
+        self.volumes = list(volumes)  # keeps the tensors alive
+        self._vols = (L.Volume * len(self.volumes))(*[wrap_volume(v) for v in self.volumes])
+        self._blocks = (C.c_uint32 * len(self.volumes))(*[int(b) for b in blocks])
+        self._jobs = (L.BatchJob * len(jobs))(*[L.BatchJob(int(v), float(i)) for v, i in jobs])
+        self.njobs = len(jobs)
+        opts = options if options is not None else extract_options()
+        d = L.BatchDesc()
+        d.volumeCount = len(self.volumes)
+        d.jobCount = self.njobs
+        d.volumes = self._vols
+        d.blockEdges = self._blocks
+        d.jobs = self._jobs
+        d.maxActiveBlocks = max_active_blocks
+        d.vertexCapacity = vertex_capacity
+        d.triangleCapacity = triangle_capacity
+        d.vertexFormat = opts.vertexFormat
+        d.frame = opts.frame
+        d.normals = opts.normals
+        d.useGraph = 1 if use_graph else 0
+        self.handle = C.c_void_p()
+        L.check(L.lib().mtx_batch_create(ctx.handle, C.byref(d), C.byref(self.handle)), "mtx_batch_create",
+                ctx.handle)
+        self.out = L.BatchOutputs()
+        L.check(L.lib().mtx_batch_get_outputs(self.handle, C.byref(self.out)), "mtx_batch_get_outputs")
+
+    def run(self):
+        L.check(L.lib().mtx_batch_run(self.handle), "mtx_batch_run", self.ctx.handle)
+
+    def results(self, check: bool = True):
+        """(per-job results as dicts, totals dict); waits for the last run."""
+        res = (L.BatchJobResult * self.njobs)()
+        tot = L.BatchTotals()
+        st = L.lib().mtx_batch_read_results(self.handle, C.cast(res, C.c_void_p), C.byref(tot))
+        if check:
+            L.check(st, "mtx_batch_read_results", self.ctx.handle)
+        jobs = [{f: getattr(r, f) for f, _ in L.BatchJobResult._fields_} for r in res]
+        totals = {f: getattr(tot, f) for f, _ in L.BatchTotals._fields_}
+        return jobs, totals
+
+    def mesh(self, r: dict):
+        """Views of one job's vertices [V, 3|8], indices [T, 3] (relative to the
+        job's first vertex) and meshlet descriptors [M, 4]."""
+        w = self.out.vertexStride // 4
+        v = device_view(self.out.vertexBuffer.ptr + 4 * w * r["vertexOffset"], (r["vertexCount"], w), torch.float32)
+        i = device_view(self.out.indexBuffer.ptr + 4 * r["indexOffset"], (r["indexCount"] // 3, 3), torch.int32)
+        m = device_view(self.out.meshletDescriptorBuffer.ptr + 16 * r["meshletOffset"], (r["meshletCount"], 4),
+                        torch.int32)
+        return v, i, m
+
+    def close(self):
+        if self.handle:
+            L.lib().mtx_batch_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
