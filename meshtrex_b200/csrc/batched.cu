@@ -443,32 +443,35 @@ __device__ __forceinline__ void batch_bases(const BatchArgs &a, uint32_t n, uint
 }
 
 // ------------------------------------------------------------ per block
-template <typename T>
+// The tile of every block is staged as float whatever the volume's dtype
+// (exact for uint8 and uint16: the same compares and interpolation bits as
+// the single-volume kernels), so one copy of each block body serves all
+// dtypes and the kernel's instruction footprint stays small.
 __device__ __forceinline__ void batch_count_block(const BatchArgs &a, const Problem &p, const WPlan &pl,
-                                                  unsigned char *ws, const uint8_t *ntab, uint32_t id, uint32_t r,
-                                                  uint32_t &parity) {
-    const Geo g = block_geo(id, p, false, sizeof(T));
-    tile_wait<T, false>(p, pl, ws, 0, g, parity, &a.ctrl->status);
-    count_block<T>(p, pl, ws, 0, g, ntab, nullptr, a.desc + r, a.faces + (uint64_t)r * a.face_stride);
+                                                  unsigned char *ws, const uint8_t *ntab, uint32_t id, uint32_t r) {
+    const Geo g = block_geo(id, p, false, 4);
+    tile_load_float(p, pl, reinterpret_cast<float *>(ws + pl.off_tile[0]), g);
+    count_block<float>(p, pl, ws, 0, g, ntab, nullptr, a.desc + r, a.faces + (uint64_t)r * a.face_stride);
 }
 
-template <typename T, int CPL, bool GENERIC>
+template <int CPL, bool GENERIC>
 __device__ __forceinline__ void batch_emit_block(const BatchArgs &a, const Problem &p, const WPlan &pl,
                                                  unsigned char *ws, const uint64_t *tab, const uint8_t *ntab,
                                                  const uint8_t *owner, uint32_t id, uint32_t r, uint64_t rank_off,
-                                                 const mtx_batch_job_result &jr, uint32_t &parity) {
-    const Geo g = block_geo(id, p, false, sizeof(T));
+                                                 const mtx_batch_job_result &jr) {
+    const Geo g = block_geo(id, p, false, 4);
     const uint4 q = __ldcg(reinterpret_cast<const uint4 *>(a.desc + r));
     const mtx_meshlet_descriptor d{q.x, q.y, q.z, q.w};
     const uint32_t nb_rk = neighbour_rank<false>(p, g, id, a.rank_pool + rank_off);
     const uint32_t nb_vb = nb_rk != kNoVertex ? __ldcg(&a.desc[nb_rk].vertexOffset) : kNoVertex;
     uint32_t rec[CPL];
     gather_issue<CPL, false>(p, pl, g, nb_rk, a.faces, a.face_stride, rec);
-    tile_wait<T, false>(p, pl, ws, 0, g, parity, &a.ctrl->status);
+    tile_load_float(p, pl, reinterpret_cast<float *>(ws + pl.off_tile[0]), g);
     gather_finish<CPL>(pl, nb_vb, rec, ws);
     void *verts = a.vertices ? (void *)((char *)a.vertices + jr.vertexOffset * a.vsz) : nullptr;
-    emit_block<T, GENERIC>(p, pl, ws, 0, g, d, tab, ntab, owner, a.indices + jr.indexOffset, jr.indexCount / 3u,
-                           verts, jr.vertexCount, a.vfmt, a.frame, a.normals, &a.ctrl->status, r);
+    emit_block<float, GENERIC, true>(p, pl, ws, 0, g, d, tab, ntab, owner, a.indices + jr.indexOffset,
+                                     jr.indexCount / 3u, verts, jr.vertexCount, a.vfmt, a.frame, a.normals,
+                                     &a.ctrl->status, r);
 }
 
 // ------------------------------------------------------------ the kernel
@@ -493,7 +496,6 @@ __global__ void __launch_bounds__(kBThreads) batch_extract_kernel(const __grid_c
     __syncthreads();
     BCtrl *ctrl = a.ctrl;
     DevStatus *st = &ctrl->status;
-    uint32_t parity = 0;
 
     // filter + ordered compaction
     for (;;) {
@@ -523,11 +525,7 @@ __global__ void __launch_bounds__(kBThreads) batch_extract_kernel(const __grid_c
             Problem p = v.p;
             p.iso = job.iso;
             const WPlan pl = v.pl;
-            switch (p.dtype) {
-            case MTX_DTYPE_U8: batch_count_block<uint8_t>(a, p, pl, ws, ntab, id, r, parity); break;
-            case MTX_DTYPE_U16: batch_count_block<uint16_t>(a, p, pl, ws, ntab, id, r, parity); break;
-            default: batch_count_block<float>(a, p, pl, ws, ntab, id, r, parity); break;
-            }
+            batch_count_block(a, p, pl, ws, ntab, id, r);
             ++done;
         }
     }
@@ -575,17 +573,7 @@ __global__ void __launch_bounds__(kBThreads) batch_extract_kernel(const __grid_c
             jr.indexOffset = __ldcg(&a.res[j].indexOffset);
             jr.vertexCount = __ldcg(&a.res[j].vertexCount);
             jr.indexCount = __ldcg(&a.res[j].indexCount);
-            switch (p.dtype) {
-            case MTX_DTYPE_U8:
-                batch_emit_block<uint8_t, CPL, GENERIC>(a, p, pl, ws, tab, ntab, owner, id, r, job.rank_off, jr, parity);
-                break;
-            case MTX_DTYPE_U16:
-                batch_emit_block<uint16_t, CPL, GENERIC>(a, p, pl, ws, tab, ntab, owner, id, r, job.rank_off, jr, parity);
-                break;
-            default:
-                batch_emit_block<float, CPL, GENERIC>(a, p, pl, ws, tab, ntab, owner, id, r, job.rank_off, jr, parity);
-                break;
-            }
+            batch_emit_block<CPL, GENERIC>(a, p, pl, ws, tab, ntab, owner, id, r, job.rank_off, jr);
         }
     }
 }
@@ -709,16 +697,15 @@ mtx_status mtx_batch_create(mtx_context_t c, const mtx_batch_desc *d, mtx_batch_
     b->vsz = d->vertexFormat == MTX_VERTEX_DATA ? 32u : 12u;
 
     // volume table, warp layout, min/max warps
-    uint32_t Bmax = 2, esz_max = 1;
+    uint32_t Bmax = 2;
     for (uint32_t v = 0; v < b->nvol; ++v) {
         rs = check_volume(c, &d->volumes[v]);
         if (rs != MTX_OK) { batch_release(b); return rs; }
         const uint32_t B = d->blockEdges[v];
         if (B < 2 || B > 16) { batch_release(b); return fail(c, MTX_ERR_INVALID_ARG, "batch: block edge outside 2..16"); }
         Bmax = std::max(Bmax, B);
-        esz_max = std::max(esz_max, dtype_size(d->volumes[v].dtype));
     }
-    const WPlan L = make_wplan(Bmax, esz_max, false, true, true);
+    const WPlan L = make_wplan(Bmax, 4, false, true, true);  // float tiles
     std::vector<BVol> vols(b->nvol);
     uint64_t leaf_total = 0, want = (uint64_t)c->sm_count * 48;
     for (uint32_t v = 0; v < b->nvol; ++v) {
@@ -737,7 +724,7 @@ mtx_status mtx_batch_create(mtx_context_t c, const mtx_batch_desc *d, mtx_batch_
         p.GY = ceil_div(p.Y, B);
         p.GZ = ceil_div(p.Z, B);
         p.nblocks = (uint64_t)p.GX * p.GY * p.GZ;
-        bv.pl = plan_in_layout(B, esz, L);
+        bv.pl = plan_in_layout(B, 4, L);
         bv.vec = ((uintptr_t)p.vol % 16 == 0) && (((uint64_t)p.X * esz) % 16 == 0) && (B == 4 || B == 8 || B == 16);
         bv.leaf_off = leaf_total;
         leaf_total += align4(p.nblocks);

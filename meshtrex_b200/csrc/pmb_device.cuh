@@ -188,6 +188,41 @@ __device__ __forceinline__ bool tile_wait(const Problem &p, const WPlan &pl, uns
     return true;
 }
 
+// Plain loads of a block's (B+1)^3 tile from a volume of run-time dtype
+// p.dtype, stored as float (exact for uint8 and uint16), so that one set of
+// block bodies serves every dtype.
+template <typename S>
+__device__ __forceinline__ void tile_load_float_from(const Problem &p, const WPlan &pl, float *tile, const Geo &g) {
+    constexpr uint32_t kLdgBatch = 8;
+    const S *vol = reinterpret_cast<const S *>(p.vol);
+    const uint32_t n = pl.B1 * pl.B1 * pl.B1;
+    for (uint32_t i0 = 0; i0 < n; i0 += 32 * kLdgBatch) {
+        float v[kLdgBatch];
+        uint32_t dst[kLdgBatch];
+#pragma unroll
+        for (uint32_t k = 0; k < kLdgBatch; ++k) {
+            const uint32_t i = i0 + k * 32 + (threadIdx.x & 31);
+            const uint32_t iq = fdiv(i, pl.rB1);
+            const uint32_t x = i - iq * pl.B1, z = fdiv(iq, pl.rB1), y = iq - z * pl.B1;
+            const uint32_t gx = g.ox + x, gy = g.oy + y, gz = g.oz + z;
+            v[k] = 0.0f;
+            dst[k] = i < n ? (z * pl.B1 + y) * pl.PX + x : 0xffffffffu;
+            if (i < n && gx < p.X && gy < p.Y && gz < p.Z)
+                v[k] = Vox<S>::val(__ldg(vol + ((uint64_t)gz * p.Y + gy) * p.X + gx));
+        }
+#pragma unroll
+        for (uint32_t k = 0; k < kLdgBatch; ++k)
+            if (dst[k] != 0xffffffffu) tile[dst[k]] = v[k];
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ void tile_load_float(const Problem &p, const WPlan &pl, float *tile, const Geo &g) {
+    if (p.dtype == MTX_DTYPE_U8) tile_load_float_from<uint8_t>(p, pl, tile, g);
+    else if (p.dtype == MTX_DTYPE_U16) tile_load_float_from<uint16_t>(p, pl, tile, g);
+    else tile_load_float_from<float>(p, pl, tile, g);
+}
+
 // Waits (bounded) for a prefetched tile that will not be used, so that no
 // copy into this warp's shared memory is in flight when it leaves.
 template <bool TMA>
@@ -430,6 +465,14 @@ __device__ __noinline__ float3 vertex_normal(const Problem &p, uint32_t gx, uint
     return n;
 }
 
+// vertex_normal for a volume whose dtype is known only at run time (p.dtype).
+static __device__ __noinline__ float3 vertex_normal_any(const Problem &p, uint32_t gx, uint32_t gy, uint32_t gz,
+                                                        uint32_t a, float t) {
+    if (p.dtype == MTX_DTYPE_U8) return vertex_normal<uint8_t>(p, gx, gy, gz, a, t);
+    if (p.dtype == MTX_DTYPE_U16) return vertex_normal<uint16_t>(p, gx, gy, gz, a, t);
+    return vertex_normal<float>(p, gx, gy, gz, a, t);
+}
+
 // Position of the vertex on the +axis edge of block voxel (x,y,z); its edge
 // parameter goes to *tout.
 template <typename T>
@@ -458,8 +501,9 @@ __device__ __forceinline__ float3 vertex_pos(const Problem &p, const WPlan &pl, 
 // kJobWin jobs; the warp then resolves the window 32 vertices at a time, one
 // per lane, staging positions in shared memory for coalesced stores.
 // GENERIC selects the VertexData / NDC / normals options; the plain form
-// writes xyz in the voxel frame.
-template <typename T, bool GENERIC>
+// writes xyz in the voxel frame.  ANY: the tile holds the voxels converted to
+// T = float and the volume's own dtype is p.dtype (used for the normals).
+template <typename T, bool GENERIC, bool ANY = false>
 __device__ __forceinline__ void emit_vertices(const Problem &p, const WPlan &pl, unsigned char *ws, uint32_t buf,
                                               const Geo &g, uint32_t vbase, uint32_t nv, void *vertices, uint32_t vfmt,
                                               uint32_t frame, uint32_t normals) {
@@ -507,7 +551,10 @@ __device__ __forceinline__ void emit_vertices(const Problem &p, const WPlan &pl,
                     stage[3 * lane + 2] = pos.z;
                 } else {
                     float3 nn = make_float3(0.0f, 0.0f, 0.0f);
-                    if (normals) nn = vertex_normal<T>(p, g.ox + x, g.oy + y, g.oz + z, a, t);
+                    if (normals) {
+                        if constexpr (ANY) nn = vertex_normal_any(p, g.ox + x, g.oy + y, g.oz + z, a, t);
+                        else nn = vertex_normal<T>(p, g.ox + x, g.oy + y, g.oz + z, a, t);
+                    }
                     float4 *v = reinterpret_cast<float4 *>(vertices) + 2ull * (vbase + w0 + b + lane);
                     v[0] = make_float4(pos.x, pos.y, pos.z, 1.0f);
                     v[1] = make_float4(nn.x, nn.y, nn.z, 0.0f);
@@ -742,7 +789,8 @@ __device__ __forceinline__ void count_block(const Problem &p, const WPlan &pl, u
 
 // Emit body of one block whose tile is staged and whose context layer has
 // been gathered: its own vertices (when `vertices` is set) and its triangles.
-template <typename T, bool GENERIC>
+// ANY as in emit_vertices.
+template <typename T, bool GENERIC, bool ANY = false>
 __device__ __forceinline__ void emit_block(const Problem &p, const WPlan &pl, unsigned char *ws, uint32_t buf,
                                            const Geo &g, const mtx_meshlet_descriptor &d, const uint64_t *tab,
                                            const uint8_t *ntab, const uint8_t *owner, uint32_t *indices,
@@ -769,7 +817,7 @@ __device__ __forceinline__ void emit_block(const Problem &p, const WPlan &pl, un
     if (lane == 0 && (bnv != d.vertexCount || bnt != d.primitiveCount))
         report(st, MTX_ERR_INTERNAL, kSiteEmitNeighbour, r, 2);
     if (vertices && bnv)
-        emit_vertices<T, GENERIC>(p, pl, ws, buf, g, d.vertexOffset, bnv, vertices, vfmt, frame, normals);
+        emit_vertices<T, GENERIC, ANY>(p, pl, ws, buf, g, d.vertexOffset, bnv, vertices, vfmt, frame, normals);
     // triangles in canonical order: each lane walks the mixed cells of its rows
     // and writes one job per triangle (cell | t << 12 | case << 16) at the
     // triangle's own position in a window of kJobWin jobs; the warp resolves
