@@ -284,6 +284,34 @@ mtx_status mtx_extract_plain_async(mtx_context_t ctx, const mtx_volume *vol,
                                    const mtx_push_constants *pc, const mtx_extract_options *opts,
                                    const mtx_mesh_buffers *out);
 
+/* ------------------------------------------------------------ adjoint */
+
+typedef enum mtx_adjoint_mode {
+    MTX_ADJOINT_ATOMIC = 0,       /* dL/dfield by FP32 atomics: summation order varies between runs */
+    MTX_ADJOINT_DETERMINISTIC = 1 /* per-block partial sums reduced in a fixed order: bitwise reproducible */
+} mtx_adjoint_mode;
+
+/* Adjoint of the extraction with the topology held fixed (meshtrex has no
+ * backward pass).  Every vertex lies on a cut edge (a, b) at
+ * p = a + t * axis with t = (iso - f(a)) / (f(b) - f(a)), which is recomputed
+ * from the volume, not stored.  Given dL/dvertex it writes the dense
+ * dL/dfield (every voxel; zero away from the surface) and dL/diso:
+ *   dL/df(a) += g * (iso - f(b)) / (f(b) - f(a))^2
+ *   dL/df(b) += g * (f(a) - iso) / (f(b) - f(a))^2
+ *   dL/diso  += g / (f(b) - f(a))
+ * with g the gradient of the vertex coordinate along the edge (vertices
+ * whose |f(b) - f(a)| <= 1e-5 sit at t = 0.5 and have no gradient).
+ * filt and meshlets come from the forward extraction of the same volume and
+ * push constants (the count must have been read back); dl_dvertex holds
+ * vertexStride floats per vertex with the position gradient first, in the
+ * forward's frame.  The output buffers are device memory, overwritten.  A
+ * block whose topology no longer matches its meshlet descriptor makes the
+ * call fail with MTX_ERR_INTERNAL at mtx_synchronize. */
+mtx_status mtx_extract_backward(mtx_context_t ctx, const mtx_volume *vol, const mtx_push_constants *pc,
+                                const mtx_filtering_output *filt, const mtx_meshlet_descriptor *meshlets,
+                                uint32_t vertexCount, const float *dl_dvertex, uint32_t vertexStride,
+                                uint32_t frame, float *dl_dfield, float *dl_diso, uint32_t mode);
+
 /* ------------------------------------------------------------ batches */
 
 /* Many extractions in one go: any number of device-resident volumes (mixed

@@ -20,6 +20,7 @@ DTYPE_U8, DTYPE_U16, DTYPE_F32 = 0, 1, 2
 VERTEX_XYZ, VERTEX_DATA = 0, 1
 FRAME_VOXEL, FRAME_NDC = 0, 1
 STAGING_AUTO, STAGING_TMA, STAGING_LDG = 0, 1, 2
+ADJOINT_ATOMIC, ADJOINT_DETERMINISTIC = 0, 1
 MAX_MIP_LEVELS = 32
 
 
@@ -150,6 +151,8 @@ SIGNATURES = [
     ("mtx_extraction_free", _ST, [_P, C.POINTER(ExtractionOutput)]),
     ("mtx_extract_plain_async", _ST, [_P, C.POINTER(Volume), C.POINTER(PushConstants),
                                       C.POINTER(ExtractOptions), C.POINTER(MeshBuffers)]),
+    ("mtx_extract_backward", _ST, [_P, C.POINTER(Volume), C.POINTER(PushConstants), C.POINTER(FilteringOutput),
+                                   _P, C.c_uint32, _P, C.c_uint32, C.c_uint32, _P, _P, C.c_uint32]),
     ("mtx_batch_create", _ST, [_P, C.POINTER(BatchDesc), C.POINTER(_P)]),
     ("mtx_batch_run", _ST, [_P]),
     ("mtx_batch_get_outputs", _ST, [_P, C.POINTER(BatchOutputs)]),

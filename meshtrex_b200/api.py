@@ -294,6 +294,24 @@ def extract_meshlet_descriptors(ctx: Context, mm: MinMax, f: Filtering, pc: L.Pu
     return Extraction(ctx, out)
 
 
+def extract_backward(ctx: Context, volume: L.Volume, pc: L.PushConstants, f: Filtering, meshlets_ptr: int,
+                     vertex_count: int, dl_dvertex: torch.Tensor, frame=L.FRAME_VOXEL,
+                     mode=L.ADJOINT_ATOMIC):
+    """mtx_extract_backward: dL/dvertex (float32 [V, 3] or [V, 8], the forward's
+    frame) -> (dL/dfield as a float32 [z, y, x] tensor, dL/diso as a float32 [1])."""
+    X, Y, Z = volume.dims[0], volume.dims[1], volume.dims[2]
+    dfield = torch.empty((Z, Y, X), dtype=torch.float32, device="cuda")
+    diso = torch.empty(1, dtype=torch.float32, device="cuda")
+    g = dl_dvertex.contiguous()
+    L.check(L.lib().mtx_extract_backward(ctx.handle, C.byref(volume), C.byref(pc), C.byref(f.out),
+                                         C.c_void_p(meshlets_ptr or 0), int(vertex_count),
+                                         C.c_void_p(g.data_ptr() if g.numel() else 0), int(g.shape[1]),
+                                         int(frame), C.c_void_p(dfield.data_ptr()), C.c_void_p(diso.data_ptr()),
+                                         int(mode)),
+            "mtx_extract_backward", ctx.handle)
+    return dfield, diso
+
+
 @dataclass
 class Mesh:
     vertices: torch.Tensor   # float32 [V, 3] or [V, 8]

@@ -14,22 +14,6 @@
 
 using namespace mtx;
 
-namespace {
-
-// Switches to the context's device for the duration of a call.
-struct DeviceGuard {
-    int prev = -1;
-    bool changed = false;
-    explicit DeviceGuard(int dev) {
-        if (cudaGetDevice(&prev) == cudaSuccess && prev != dev) changed = cudaSetDevice(dev) == cudaSuccess;
-    }
-    ~DeviceGuard() {
-        if (changed) cudaSetDevice(prev);
-    }
-};
-
-}  // namespace
-
 struct mtx_profiler {
     mtx_context *ctx = nullptr;
     struct Region {
@@ -207,7 +191,7 @@ void prof_end(mtx_profiler *p, cudaStream_t s) {
     p->open_a = nullptr;
 }
 
-static Problem make_problem(const mtx_volume *v, uint32_t B, float iso) {
+Problem make_problem(const mtx_volume *v, uint32_t B, float iso) {
     Problem p;
     p.vol = v->data.ptr;
     p.X = v->dims[0];
@@ -286,7 +270,8 @@ mtx_status mtx_context_destroy(mtx_context_t c) {
     if (!c) return MTX_ERR_INVALID_ARG;
     DeviceGuard g(c->device);
     cudaStreamSynchronize(c->stream);
-    for (Scratch *s : {&c->filter_status, &c->count_status, &c->faces, &c->leaf, &c->ids, &c->rank, &c->desc, &c->misc})
+    for (Scratch *s : {&c->filter_status, &c->count_status, &c->faces, &c->leaf, &c->ids, &c->rank, &c->desc, &c->misc,
+                       &c->adj_partial, &c->adj_iso})
         dev_free(s->ptr);
     cudaFree(c->ctrl);
     cudaFreeHost(c->pinned);

@@ -664,25 +664,12 @@ mtx_status batch_enqueue(mtx_batch *b, cudaStream_t s) {
 
 }  // namespace
 
-struct DeviceScope {
-    int prev = -1;
-    explicit DeviceScope(int d) {
-        cudaGetDevice(&prev);
-        if (prev != d) cudaSetDevice(d);
-    }
-    ~DeviceScope() {
-        int cur = -1;
-        cudaGetDevice(&cur);
-        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
-    }
-};
-
 extern "C" {
 
 mtx_status mtx_batch_create(mtx_context_t c, const mtx_batch_desc *d, mtx_batch_t *out) {
     if (!c || !d || !out) return MTX_ERR_INVALID_ARG;
     *out = nullptr;
-    DeviceScope dg(c->device);
+    DeviceGuard dg(c->device);
     if (d->volumeCount == 0 || d->jobCount == 0 || !d->volumes || !d->blockEdges || !d->jobs)
         return fail(c, MTX_ERR_INVALID_ARG, "batch: empty volume or job list");
     if (d->vertexFormat > MTX_VERTEX_DATA || d->frame > MTX_FRAME_NDC)
@@ -863,7 +850,7 @@ mtx_status mtx_batch_create(mtx_context_t c, const mtx_batch_desc *d, mtx_batch_
 mtx_status mtx_batch_run(mtx_batch_t b) {
     if (!b) return MTX_ERR_INVALID_ARG;
     mtx_context *c = b->ctx;
-    DeviceScope dg(c->device);
+    DeviceGuard dg(c->device);
     if (!b->use_graph) return batch_enqueue(b, c->stream);
     if (!b->exec) {
         if (!b->capture_stream) MTX_CUDA(c, cudaStreamCreateWithFlags(&b->capture_stream, cudaStreamNonBlocking));
@@ -897,7 +884,7 @@ mtx_status mtx_batch_get_outputs(mtx_batch_t b, mtx_batch_outputs *o) {
 mtx_status mtx_batch_read_results(mtx_batch_t b, mtx_batch_job_result *results, mtx_batch_totals *totals) {
     if (!b) return MTX_ERR_INVALID_ARG;
     mtx_context *c = b->ctx;
-    DeviceScope dg(c->device);
+    DeviceGuard dg(c->device);
     MTX_CUDA(c, cudaStreamSynchronize(c->stream));
     if (results)
         MTX_CUDA(c, cudaMemcpy(results, b->args.res, sizeof(mtx_batch_job_result) * b->njobs, cudaMemcpyDeviceToHost));
@@ -918,7 +905,7 @@ mtx_status mtx_batch_read_results(mtx_batch_t b, mtx_batch_job_result *results, 
 
 mtx_status mtx_batch_destroy(mtx_batch_t b) {
     if (!b) return MTX_ERR_INVALID_ARG;
-    DeviceScope dg(b->ctx->device);
+    DeviceGuard dg(b->ctx->device);
     batch_release(b);
     return MTX_OK;
 }

@@ -43,6 +43,7 @@ struct mtx_context {
     mtx::Ctrl *ctrl = nullptr;   // device
     uint32_t *pinned = nullptr;  // pinned host words for count readbacks
     mtx::Scratch filter_status, count_status, faces, leaf, ids, rank, desc, misc;
+    mtx::Scratch adj_partial, adj_iso;  // adjoint: per-block partial tiles and isovalue sums
     mtx_profiler *prof = nullptr;  // records stage times of calls given no profiler
     mtx_tuning tuning = {0, 0, 0, 0};
 };
@@ -50,6 +51,18 @@ struct mtx_context {
 namespace mtx {
 
 // ------------------------------------------------------------ helpers
+// Makes `dev` current for the scope of a call and restores the caller's device.
+struct DeviceGuard {
+    int prev = -1;
+    bool changed = false;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) == cudaSuccess && prev != dev) changed = cudaSetDevice(dev) == cudaSuccess;
+    }
+    ~DeviceGuard() {
+        if (changed) cudaSetDevice(prev);
+    }
+};
+
 mtx_status fail(mtx_context *c, mtx_status s, const std::string &msg);
 mtx_status cuda_fail(mtx_context *c, cudaError_t e, const char *what);
 #define MTX_CUDA(c, call)                                  \
@@ -65,6 +78,13 @@ mtx_status scratch_reserve(mtx_context *c, Scratch &s, size_t bytes);
 inline uint32_t dtype_size(uint32_t dt) { return dt == MTX_DTYPE_U8 ? 1u : dt == MTX_DTYPE_U16 ? 2u : 4u; }
 inline uint64_t nvox(const uint32_t d[3]) { return (uint64_t)d[0] * d[1] * d[2]; }
 inline uint32_t ceil_div(uint32_t a, uint32_t b) { return (a + b - 1) / b; }
+
+// The kernels' view of a volume, block edge and isovalue.
+struct Problem;
+Problem make_problem(const mtx_volume *v, uint32_t B, float iso);
+// Profiler regions around the launches of a call (no-ops for a null profiler).
+void prof_begin(mtx_profiler *p, const char *name, cudaStream_t s);
+void prof_end(mtx_profiler *p, cudaStream_t s);
 
 // Validate a volume + push constants pair (cubic block edge in [2, 16]).
 mtx_status check_volume(mtx_context *c, const mtx_volume *v);
