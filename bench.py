@@ -339,6 +339,9 @@ def run_mtx(args):
         del exts
         line["batched"] = run_batched(ctx, stream, steps=max(3, min(20, steps)))
 
+    if not args.no_backward:
+        line["backward"] = run_backward(ctx, stream, steps=max(3, min(20, steps)))
+
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -541,6 +544,84 @@ def run_batched(ctx, stream, steps):
     return out
 
 
+def run_backward(ctx, stream, steps):
+    """The differentiation workload: 512^3 float32 torus SDF (R 0.3, r 0.1) +
+    0.05 fBm (seed 4), isovalue 0, block 8^3.  Forward = the whole plain
+    extraction (asynchronous call: min/max, octree, filter, count, emit);
+    backward = mtx_extract_backward from dL/dvertex of the loss
+    mean_v (|v - c| - 0.35)^2 (v in [0, 1] coordinates) to the dense
+    dL/dfield and dL/diso, in both modes.  Device times with CUDA events."""
+    import ctypes as C
+
+    from meshtrex_b200 import _lib as L
+    from meshtrex_b200 import api, synth
+    n, block, iso = 512, 8, 0.0
+    vol = synth.torus(n, seed=4, device="cuda")
+    torch.cuda.synchronize()
+    v = api.wrap_volume(vol)
+    pc = api.push_constants((n, n, n), block, iso)
+    mm = api.compute_min_max_mip(ctx, v, pc)
+    f = api.filter_active_blocks(ctx, mm, pc)
+    nact = api.read_active_block_count(ctx, f)
+    x = api.extract_meshlet_descriptors(ctx, mm, f, pc)
+    V, T = x.vertex_count, x.index_count // 3
+    verts = x.vertices().requires_grad_(True)
+    loss = ((verts / (n - 1) - 0.5).norm(dim=1) - 0.35).pow(2).mean()
+    (gv,) = torch.autograd.grad(loss, [verts])
+    gv = gv.contiguous()
+    fwd = api.AsyncExtractor(ctx, vol, block, iso, V + 1024, T + 1024, max_active_blocks=nact + 1024)
+    dfield = torch.empty((n, n, n), dtype=torch.float32, device="cuda")
+    diso = torch.empty(1, dtype=torch.float32, device="cuda")
+
+    def bwd(mode):
+        L.check(L.lib().mtx_extract_backward(ctx.handle, C.byref(v), C.byref(pc), C.byref(f.out),
+                                             C.c_void_p(x.out.meshletDescriptorBuffer.ptr), V,
+                                             C.c_void_p(gv.data_ptr()), 3, L.FRAME_VOXEL,
+                                             C.c_void_p(dfield.data_ptr()), C.c_void_p(diso.data_ptr()), mode),
+                "mtx_extract_backward", ctx.handle)
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    t_fwd = timed(fwd.run)
+    t_atomic = timed(lambda: bwd(L.ADJOINT_ATOMIC))
+    t_det = timed(lambda: bwd(L.ADJOINT_DETERMINISTIC))
+    ctx.synchronize()
+    c = fwd.counters.cpu().numpy().view(np.uint32)
+    assert int(c[4]) == 0 and int(c[0]) == V
+    nvox = n ** 3
+    bwd_bytes = 12 * V + 2 * 4 * V + 4 * nvox
+    fwd_bytes = 4 * nvox + 12 * V + 12 * T
+    peak, peak_kind = peak_hbm()
+    out = {
+        "workload": "512^3 float32 torus SDF (R 0.3, r 0.1) + 0.05 fBm (4 octaves, seed 4), isovalue 0, block 8^3; "
+                    "loss mean_v (|v - c| - 0.35)^2",
+        "vertices": V, "triangles": T, "active_blocks": nact,
+        "ms_forward": t_fwd, "ms_backward_atomic": t_atomic, "ms_backward_deterministic": t_det,
+        "bwd_fwd_ratio_atomic": t_atomic / t_fwd, "bwd_fwd_ratio_deterministic": t_det / t_fwd,
+        "forward_gbs": fwd_bytes / (t_fwd / 1000.0) / 1e9,
+        "roofline": {"bound": "hbm", "achieved": bwd_bytes / (t_atomic / 1000.0) / 1e9, "peak": peak,
+                     "unit": "GB/s", "frac": bwd_bytes / (t_atomic / 1000.0) / 1e9 / peak,
+                     "algorithmic_bytes": bwd_bytes, "peak_kind": peak_kind,
+                     "what": "atomic mode: 12 B/vertex dL/dvertex read + 2 x 4 B edge endpoints + 4 B/voxel dL/dfield"},
+        "steps": steps,
+    }
+    x.free()
+    f.free()
+    mm.free()
+    del fwd, dfield, vol
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -550,6 +631,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 64-volume leg")
+    ap.add_argument("--no-backward", action="store_true", help="skip the backward (adjoint) leg")
     ap.add_argument("--size", type=int, default=1024, help="volume edge (profiling runs only)")
     ap.add_argument("--cache", default="", help="raw file to read/write the generated volume")
     args = ap.parse_args()
