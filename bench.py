@@ -337,7 +337,7 @@ def run_mtx(args):
 
     if not args.no_batch:
         del exts
-        line["batched"] = run_batched(ctx, stream, steps=max(3, min(20, steps)))
+        line["batched"] = run_batched(ctx, stream, steps=max(3, min(20, steps)), scale_down=args.batch_scale)
 
     if not args.no_backward:
         line["backward"] = run_backward(ctx, stream, steps=max(3, min(20, steps)))
@@ -424,7 +424,7 @@ def run_e2e(ctx, vol_dev, ws, steps):
                     "readActiveBlockCount -> extractMeshletDescriptors -> mesh copied to pinned host memory"}
 
 
-def run_batched(ctx, stream, steps):
+def run_batched(ctx, stream, steps, scale_down=1):
     """The 64-volume mix (anisotropic edges from {64..512}, uint8/uint16/float32,
     1-16 isovalues each, seed 3): one batched run per step (a CUDA graph of the
     batched min/max and the persistent extraction kernel) against the same
@@ -432,7 +432,7 @@ def run_batched(ctx, stream, steps):
     and recorded into a CUDA graph.  Per-job outputs are compared bit for bit."""
     from meshtrex_b200 import api, synth
     t_gen = time.perf_counter()
-    items = synth.batch(seed=3, n=64, device="cuda")
+    items = synth.batch(seed=3, n=64, device="cuda", scale_down=scale_down)
     torch.cuda.synchronize()
     t_gen = time.perf_counter() - t_gen
     vols = [it.volume for it in items]
@@ -519,7 +519,8 @@ def run_batched(ctx, stream, steps):
     peak, peak_kind = peak_hbm()
     out = {
         "workload": "64 volumes (edges from {64,96,128,192,256,384,512} per axis, uint8/uint16/float32 Gaussian "
-                    "blobs, seed 3), 1-16 isovalues each in the 10th-90th percentile; block 8^3",
+                    "blobs, seed 3), 1-16 isovalues each in the 10th-90th percentile; block 8^3"
+                    + (f"; edges divided by {scale_down}" if scale_down > 1 else ""),
         "volumes": len(vols), "jobs": len(jobs), "volume_bytes": vol_bytes, "job_voxels": job_voxels,
         "active_blocks": tot["activeBlocks"], "vertices": V, "triangles": T,
         "ms_batched": 1000.0 * t_batch, "ms_plain_launches": 1000.0 * t_plain,
@@ -632,6 +633,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 64-volume leg")
     ap.add_argument("--no-backward", action="store_true", help="skip the backward (adjoint) leg")
+    ap.add_argument("--batch-scale", type=int, default=1, help="divide the batch's volume edges (profiling runs only)")
     ap.add_argument("--size", type=int, default=1024, help="volume edge (profiling runs only)")
     ap.add_argument("--cache", default="", help="raw file to read/write the generated volume")
     args = ap.parse_args()
