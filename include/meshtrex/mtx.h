@@ -209,6 +209,19 @@ mtx_status mtx_volume_wrap(void *device_ptr, const uint32_t dims[3], uint32_t dt
                            mtx_volume *out);
 mtx_status mtx_volume_free(mtx_context_t ctx, mtx_volume *vol);
 
+/* The file-name scheme of loadVolume (src/volume.h:14-30):
+ * "<name>_<X>x<Y>x<Z>_<type>.raw" with type uint8, uint16 or float32 (also
+ * "float").  meshtrex reads every type other than uint8 as 16-bit; here an
+ * unknown type is MTX_ERR_UNSUPPORTED and a name that does not match is
+ * MTX_ERR_INVALID_ARG.  Host only. */
+mtx_status mtx_parse_volume_name(const char *path, uint32_t dims[3], uint32_t *dtype);
+/* loadVolume (src/volume.h:14-43) and the staging upload of computeMinMaxMip
+ * (src/minMaxManager.cpp:115-125) in one call: the raw file is streamed to a
+ * new device volume through two 64 MiB pinned buffers, reading one chunk
+ * while the previous one is copied.  Returns when the volume is on the
+ * device.  A file shorter than its name says is MTX_ERR_INVALID_ARG. */
+mtx_status mtx_volume_load(mtx_context_t ctx, const char *path, mtx_volume *out);
+
 /* PushConstants as src/meshtrex.cpp:76-84 fills them, for a cubic block. */
 mtx_status mtx_push_constants_init(const uint32_t dims[3], uint32_t block_edge, float isovalue,
                                    mtx_push_constants *out);
@@ -283,6 +296,33 @@ mtx_status mtx_extraction_free(mtx_context_t ctx, mtx_extraction_output *ext);
 mtx_status mtx_extract_plain_async(mtx_context_t ctx, const mtx_volume *vol,
                                    const mtx_push_constants *pc, const mtx_extract_options *opts,
                                    const mtx_mesh_buffers *out);
+
+/* ------------------------------------------------------------ export */
+
+/* readDataChunkFromBuffer / readCounterFromBuffer
+ * (src/extractionTestUtils.cpp:203-235): copies bytes from offset of a
+ * device buffer into host memory, after the work queued on the context's
+ * stream. */
+mtx_status mtx_read_buffer(mtx_context_t ctx, const mtx_buffer *src, uint64_t offset, void *host, uint64_t bytes);
+
+/* Weld check of a mesh written by mtx_write_obj. */
+typedef struct mtx_obj_stats {
+    uint32_t vertexCount;
+    uint32_t triangleCount;
+    uint32_t uniqueVertexCount;       /* distinct position (and normal) bit patterns */
+    uint32_t degenerateTriangleCount; /* triangles with two corners at the same vertex or position */
+} mtx_obj_stats;
+
+/* writeGPUExtractionToOBJ (src/extractionTestUtils.cpp:203-369) for host
+ * copies of the mesh: "v" lines, "vn" lines for the 32-byte VertexData
+ * layout (vertexStride 8 floats; 3 = xyz only), and 1-based "f" lines
+ * ("f a//a b//b c//c" with normals).  Coordinates are written with 9
+ * significant digits, so that they read back to the same float bits
+ * (meshtrex writes 6).  Like meshtrex it reports the distinct vertices and
+ * the degenerate triangles but writes the mesh as given; PMB writes every
+ * vertex once, so the vertex count and the distinct count agree. */
+mtx_status mtx_write_obj(const char *path, const float *vertices, uint32_t vertexCount, uint32_t vertexStride,
+                         const uint32_t *indices, uint32_t indexCount, mtx_obj_stats *stats);
 
 /* ------------------------------------------------------------ adjoint */
 

@@ -118,6 +118,11 @@ class BatchOutputs(C.Structure):
                 ("jobResultBuffer", Buffer), ("vertexStride", C.c_uint32), ("_pad", C.c_uint32)]
 
 
+class ObjStats(C.Structure):
+    _fields_ = [("vertexCount", C.c_uint32), ("triangleCount", C.c_uint32),
+                ("uniqueVertexCount", C.c_uint32), ("degenerateTriangleCount", C.c_uint32)]
+
+
 # (name, restype, argtypes) of every exported entry point
 _P = C.c_void_p
 _ST = C.c_int
@@ -133,6 +138,10 @@ SIGNATURES = [
     ("mtx_volume_upload", _ST, [_P, _P, C.POINTER(C.c_uint32), C.c_uint32, C.POINTER(Volume)]),
     ("mtx_volume_wrap", _ST, [_P, C.POINTER(C.c_uint32), C.c_uint32, C.POINTER(Volume)]),
     ("mtx_volume_free", _ST, [_P, C.POINTER(Volume)]),
+    ("mtx_parse_volume_name", _ST, [C.c_char_p, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
+    ("mtx_volume_load", _ST, [_P, C.c_char_p, C.POINTER(Volume)]),
+    ("mtx_read_buffer", _ST, [_P, C.POINTER(Buffer), C.c_uint64, _P, C.c_uint64]),
+    ("mtx_write_obj", _ST, [C.c_char_p, _P, C.c_uint32, C.c_uint32, _P, C.c_uint32, C.POINTER(ObjStats)]),
     ("mtx_push_constants_init", _ST, [C.POINTER(C.c_uint32), C.c_uint32, C.c_float,
                                       C.POINTER(PushConstants)]),
     ("mtx_key_to_float", C.c_float, [C.c_uint32, C.c_uint32]),

@@ -461,6 +461,16 @@ mtx_status mtx_read_active_block_count(mtx_context_t c, mtx_filtering_output *f)
     return MTX_OK;
 }
 
+mtx_status mtx_read_buffer(mtx_context_t c, const mtx_buffer *src, uint64_t offset, void *host, uint64_t bytes) {
+    if (!c || !src || (bytes && (!src->ptr || !host))) return c ? fail(c, MTX_ERR_INVALID_ARG, "null argument") : MTX_ERR_INVALID_ARG;
+    if (offset > src->size || bytes > src->size - offset) return fail(c, MTX_ERR_INVALID_ARG, "read past the buffer");
+    if (!bytes) return MTX_OK;
+    DeviceGuard g(c->device);
+    MTX_CUDA(c, cudaMemcpyAsync(host, (const char *)src->ptr + offset, bytes, cudaMemcpyDeviceToHost, c->stream));
+    MTX_CUDA(c, cudaStreamSynchronize(c->stream));
+    return MTX_OK;
+}
+
 mtx_status mtx_filtering_free(mtx_context_t c, mtx_filtering_output *f) {
     if (!c || !f) return MTX_ERR_INVALID_ARG;
     DeviceGuard g(c->device);
