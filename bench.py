@@ -342,6 +342,12 @@ def run_mtx(args):
     if not args.no_backward:
         line["backward"] = run_backward(ctx, stream, steps=max(3, min(20, steps)))
 
+    if not args.no_gyroid:
+        exts = vol = None  # release the 1024^3 volume and its outputs first
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+        line["gyroid"] = run_gyroid(ctx, stream, steps=max(3, min(10, steps)), n=args.gyroid_size)
+
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()
@@ -623,6 +629,67 @@ def run_backward(ctx, stream, steps):
     return out
 
 
+def run_gyroid(ctx, stream, steps, n=2048):
+    """The large float32 workload: n^3 gyroid sin(kx)cos(ky) + sin(ky)cos(kz) +
+    sin(kz)cos(kx), k = 2 pi 12, + N(0, 0.02) (seed 2), isovalue 0 (32 GiB at
+    2048^3).  mtx_autotune picks the block edge, warps, staging and min/max
+    slices; the chosen shape and the default one (block 8^3, default tuning)
+    are then timed with the asynchronous whole-path call."""
+    from meshtrex_b200 import _lib as L
+    from meshtrex_b200 import api, synth
+    t0 = time.perf_counter()
+    vol = synth.gyroid(n, seed=2, device="cuda")
+    torch.cuda.synchronize()
+    t_gen = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    tune = api.autotune(ctx, vol, 0.0, flags=L.AUTOTUNE_QUICK)
+    t_tune = time.perf_counter() - t0
+
+    def timed(block, tuning):
+        ctx.set_tuning(tuning["minmaxZChunk"], tuning["minmaxSlices"], tuning["extractWarps"], tuning["staging"])
+        m = api.extract(vol, block, 0.0, ctx=ctx)
+        V, T, A = m.vertices.shape[0], m.indices.shape[0], m.active_ids.shape[0]
+        del m
+        ex = api.AsyncExtractor(ctx, vol, block, 0.0, V + 1024, T + 1024, max_active_blocks=A + 1024)
+        for _ in range(2):
+            ex.run()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(steps):
+            ex.run()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ctx.synchronize()
+        c = ex.counters.cpu().numpy().view(np.uint32)
+        assert int(c[4]) == 0 and int(c[0]) == V and int(c[1]) == 3 * T
+        del ex
+        return e0.elapsed_time(e1) / steps, V, T, A
+
+    default = {"minmaxZChunk": 0, "minmaxSlices": 0, "extractWarps": 0, "staging": 0}
+    ms_tuned, V, T, A = timed(tune["blockEdge"], tune["tuning"])
+    ms_default, V8, T8, _ = timed(8, default)
+    ctx.set_tuning(0, 0, 0, 0)
+    nvox = n ** 3
+    peak, peak_kind = peak_hbm()
+    alg = 4 * nvox + 12 * V + 12 * T
+    out = {
+        "workload": f"{n}^3 float32 gyroid (k = 2 pi 12) + N(0, 0.02), seed 2, isovalue 0",
+        "autotuned": {"block": tune["blockEdge"], "tuning": tune["tuning"], "candidates": tune["candidates"],
+                      "tune_s": t_tune},
+        "ms_tuned": ms_tuned, "ms_default_b8": ms_default, "speedup_vs_default": ms_default / ms_tuned,
+        "gvoxels_per_s": nvox / ms_tuned / 1e6, "tris_per_s": T / ms_tuned * 1e3,
+        "vertices": V, "triangles": T, "active_blocks": A, "triangles_b8": T8,
+        "pipeline_roofline": {"achieved": alg / ms_tuned / 1e6, "peak": peak, "unit": "GB/s",
+                              "frac": alg / ms_tuned / 1e6 / peak, "algorithmic_bytes": alg, "peak_kind": peak_kind,
+                              "what": "volume read once + 12 B per vertex + 12 B per triangle written"},
+        "generate_s": t_gen, "steps": steps,
+    }
+    del vol
+    torch.cuda.empty_cache()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -634,6 +701,8 @@ def main():
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 64-volume leg")
     ap.add_argument("--no-backward", action="store_true", help="skip the backward (adjoint) leg")
     ap.add_argument("--batch-scale", type=int, default=1, help="divide the batch's volume edges (profiling runs only)")
+    ap.add_argument("--no-gyroid", action="store_true", help="skip the autotuned 2048^3 float32 gyroid leg")
+    ap.add_argument("--gyroid-size", type=int, default=2048, help="gyroid edge (profiling runs only)")
     ap.add_argument("--size", type=int, default=1024, help="volume edge (profiling runs only)")
     ap.add_argument("--cache", default="", help="raw file to read/write the generated volume")
     args = ap.parse_args()

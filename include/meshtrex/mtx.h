@@ -453,6 +453,32 @@ typedef struct mtx_tuning {
 mtx_status mtx_context_set_tuning(mtx_context_t ctx, const mtx_tuning *t);
 mtx_status mtx_context_get_tuning(mtx_context_t ctx, mtx_tuning *t);
 
+/* Result of mtx_autotune: pass blockEdge to mtx_push_constants_init and tuning
+ * to mtx_context_set_tuning.  The block edge changes the meshlet layout and
+ * the output order (one meshlet per block), not the surface. */
+typedef struct mtx_autotune_result {
+    uint32_t blockEdge;  /* 4, 8 or 16 */
+    mtx_tuning tuning;
+    double ms;           /* device time of one plain extraction with these choices */
+    uint32_t fromCache;  /* 1 if no candidate was timed */
+    uint32_t candidates; /* candidates timed */
+} mtx_autotune_result;
+
+#define MTX_AUTOTUNE_IGNORE_CACHE 1u /* time the candidates even if a cached choice exists */
+#define MTX_AUTOTUNE_QUICK 2u        /* one repetition per candidate instead of the best of three */
+
+/* Picks the block edge (4, 8, 16), the warps per CTA of the extraction passes
+ * (2, 4, 8), the staging (TMA or plain loads) and the min/max slices (1, 2, 4)
+ * for one volume by timing the whole plain extraction of each candidate at
+ * `isovalue` on the device.  The score is the sum of the stage times that CUDA
+ * events record.  The choice is cached per (dims, dtype, device name) in the
+ * process and, when cache_path is not NULL, appended to that text file,
+ * which later calls and processes read first.  The context's tuning is left
+ * as it was.  No meshtrex counterpart: meshtrex fixes these at compile time
+ * (extractionPipeline.cpp:238-256, pmb.task.glsl:19,27). */
+mtx_status mtx_autotune(mtx_context_t ctx, const mtx_volume *vol, float isovalue, const char *cache_path,
+                        uint32_t flags, mtx_autotune_result *out);
+
 /* Records the stage times of every later call on this context that is not
  * given its own profiler, the asynchronous whole-path call included (NULL
  * turns it off); the GPUProfiler* argument of meshtrex's managers made

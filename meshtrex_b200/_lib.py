@@ -118,6 +118,14 @@ class BatchOutputs(C.Structure):
                 ("jobResultBuffer", Buffer), ("vertexStride", C.c_uint32), ("_pad", C.c_uint32)]
 
 
+class AutotuneResult(C.Structure):
+    _fields_ = [("blockEdge", C.c_uint32), ("tuning", Tuning), ("ms", C.c_double),
+                ("fromCache", C.c_uint32), ("candidates", C.c_uint32)]
+
+
+AUTOTUNE_IGNORE_CACHE, AUTOTUNE_QUICK = 1, 2
+
+
 class ObjStats(C.Structure):
     _fields_ = [("vertexCount", C.c_uint32), ("triangleCount", C.c_uint32),
                 ("uniqueVertexCount", C.c_uint32), ("degenerateTriangleCount", C.c_uint32)]
@@ -171,6 +179,7 @@ SIGNATURES = [
     ("mtx_context_set_profiler", _ST, [_P, _P]),
     ("mtx_context_set_tuning", _ST, [_P, C.POINTER(Tuning)]),
     ("mtx_context_get_tuning", _ST, [_P, C.POINTER(Tuning)]),
+    ("mtx_autotune", _ST, [_P, C.POINTER(Volume), C.c_float, C.c_char_p, C.c_uint32, C.POINTER(AutotuneResult)]),
     ("mtx_profiler_destroy", _ST, [_P]),
     ("mtx_profiler_begin_frame", _ST, [_P]),
     ("mtx_profiler_end_frame", _ST, [_P]),

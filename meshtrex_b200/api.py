@@ -447,3 +447,15 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def autotune(ctx: Context, volume: torch.Tensor, iso: float, cache_path: str | None = None, flags: int = 0) -> dict:
+    """mtx_autotune on a CUDA volume tensor [z, y, x]: the block edge and the
+    tuning to use for it ({blockEdge, tuning: {...}, ms, fromCache, candidates})."""
+    r = L.AutotuneResult()
+    v = wrap_volume(volume)
+    L.check(L.lib().mtx_autotune(ctx.handle, C.byref(v), float(iso),
+                                 cache_path.encode() if cache_path else None, int(flags), C.byref(r)),
+            "mtx_autotune", ctx.handle)
+    t = {f: getattr(r.tuning, f) for f, _ in L.Tuning._fields_}
+    return {"blockEdge": r.blockEdge, "tuning": t, "ms": r.ms, "fromCache": r.fromCache, "candidates": r.candidates}

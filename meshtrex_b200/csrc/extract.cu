@@ -252,6 +252,10 @@ static mtx_status launch_stage(mtx_context *c, const Problem &p, const ExtractAr
     // warps per CTA: threads/32 of the options, else the context's tuning, else 4
     uint32_t W = a.threads ? a.threads / 32 : (c->tuning.extractWarps ? c->tuning.extractWarps : 4);
     W = std::min<uint32_t>(std::max<uint32_t>(W, 1), kMaxWarps);
+    // no more warps than the shared memory holds (16^3 float tiles fit 7, not 8)
+    const WPlan pl = make_wplan(p.B, dtype_size(p.dtype), tma, EMIT);
+    const uint32_t room = c->max_smem_optin > (int)kTableBytes ? (uint32_t)c->max_smem_optin - kTableBytes : 0u;
+    W = std::min<uint32_t>(W, std::max<uint32_t>(1, room / pl.bytes));
     switch (p.dtype) {
     case MTX_DTYPE_U8: return EMIT ? run_emit<uint8_t>(c, p, a, map, tma, W, s) : run_count<uint8_t>(c, p, a, map, tma, W, s);
     case MTX_DTYPE_U16: return EMIT ? run_emit<uint16_t>(c, p, a, map, tma, W, s) : run_count<uint16_t>(c, p, a, map, tma, W, s);
