@@ -27,7 +27,7 @@
 #include <vector>
 
 #include "minmax_device.cuh"
-#include "pmb_device.cuh"
+#include "pmb_balanced.cuh"
 
 namespace mtx {
 
@@ -446,12 +446,14 @@ __device__ __forceinline__ void batch_bases(const BatchArgs &a, uint32_t n, uint
 // The tile of every block is staged as float whatever the volume's dtype
 // (exact for uint8 and uint16: the same compares and interpolation bits as
 // the single-volume kernels), so one copy of each block body serves all
-// dtypes and the kernel's instruction footprint stays small.
+// dtypes and the kernel's instruction footprint stays small.  The bodies are
+// the balanced ones (pmb_balanced.cuh): batches of many volumes and
+// isovalues tend to have dense blocks.
 __device__ __forceinline__ void batch_count_block(const BatchArgs &a, const Problem &p, const WPlan &pl,
                                                   unsigned char *ws, const uint8_t *ntab, uint32_t id, uint32_t r) {
     const Geo g = block_geo(id, p, false, 4);
     tile_load_float(p, pl, reinterpret_cast<float *>(ws + pl.off_tile[0]), g);
-    count_block<float>(p, pl, ws, 0, g, ntab, nullptr, a.desc + r, a.faces + (uint64_t)r * a.face_stride);
+    count_block_balanced(p, pl, ws, g, ntab, a.desc + r, a.faces + (uint64_t)r * a.face_stride);
 }
 
 template <int CPL, bool GENERIC>
@@ -469,9 +471,8 @@ __device__ __forceinline__ void batch_emit_block(const BatchArgs &a, const Probl
     tile_load_float(p, pl, reinterpret_cast<float *>(ws + pl.off_tile[0]), g);
     gather_finish<CPL>(pl, nb_vb, rec, ws);
     void *verts = a.vertices ? (void *)((char *)a.vertices + jr.vertexOffset * a.vsz) : nullptr;
-    emit_block<float, GENERIC, true>(p, pl, ws, 0, g, d, tab, ntab, owner, a.indices + jr.indexOffset,
-                                     jr.indexCount / 3u, verts, jr.vertexCount, a.vfmt, a.frame, a.normals,
-                                     &a.ctrl->status, r);
+    emit_block_balanced<GENERIC>(p, pl, ws, g, d, tab, ntab, owner, a.indices + jr.indexOffset, jr.indexCount / 3u,
+                                 verts, jr.vertexCount, a.vfmt, a.frame, a.normals, &a.ctrl->status, r);
 }
 
 // ------------------------------------------------------------ the kernel
@@ -614,16 +615,18 @@ KernelFn batch_kernel(int variant) {
     }
 }
 
-WPlan plan_in_layout(uint32_t B, uint32_t esz, const WPlan &L) {
-    WPlan p = make_wplan(B, esz, false, true, true);
+WPlan plan_in_layout(uint32_t B, const WPlan &L) {
+    WPlan p = make_wplan_balanced(B);
     p.off_tile[0] = p.off_tile[1] = L.off_tile[0];
+    p.off_vtab = L.off_vtab;
     p.off_bar = L.off_bar;
     p.off_rows = L.off_rows;
     p.off_cross = L.off_cross;
     p.off_vp = L.off_vp;
-    p.off_tp = L.off_tp;
+    p.off_list = L.off_list;
     p.off_nvid = L.off_nvid;
     p.off_nm = L.off_nm;
+    p.off_vmsk = L.off_vmsk;
     p.off_stage = L.off_stage;
     p.off_jobs = L.off_jobs;
     p.bytes = L.bytes;
@@ -692,7 +695,7 @@ mtx_status mtx_batch_create(mtx_context_t c, const mtx_batch_desc *d, mtx_batch_
         if (B < 2 || B > 16) { batch_release(b); return fail(c, MTX_ERR_INVALID_ARG, "batch: block edge outside 2..16"); }
         Bmax = std::max(Bmax, B);
     }
-    const WPlan L = make_wplan(Bmax, 4, false, true, true);  // float tiles
+    const WPlan L = make_wplan_balanced(Bmax);  // float tile, vertex table in its place
     std::vector<BVol> vols(b->nvol);
     uint64_t leaf_total = 0, want = (uint64_t)c->sm_count * 48;
     for (uint32_t v = 0; v < b->nvol; ++v) {
@@ -711,7 +714,7 @@ mtx_status mtx_batch_create(mtx_context_t c, const mtx_batch_desc *d, mtx_batch_
         p.GY = ceil_div(p.Y, B);
         p.GZ = ceil_div(p.Z, B);
         p.nblocks = (uint64_t)p.GX * p.GY * p.GZ;
-        bv.pl = plan_in_layout(B, 4, L);
+        bv.pl = plan_in_layout(B, L);
         bv.vec = ((uintptr_t)p.vol % 16 == 0) && (((uint64_t)p.X * esz) % 16 == 0) && (B == 4 || B == 8 || B == 16);
         bv.leaf_off = leaf_total;
         leaf_total += align4(p.nblocks);
