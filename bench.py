@@ -52,6 +52,23 @@ def dist_env():
     return ws, rank, local
 
 
+def max_over_ranks(t_local: float, ws: int, device: str = "cuda") -> float:
+    """The step time of the whole job: the slowest rank's (one all-reduce; every
+    rank calls it at the same point)."""
+    if ws <= 1:
+        return t_local
+    import torch.distributed as dist
+    tt = torch.tensor([t_local], device=device, dtype=torch.float64)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
+def job_throughput(units_per_rank: float, ws: int, t_max: float) -> float:
+    """Whole-job throughput: every rank processed units_per_rank (replicas,
+    weak scaling) in the slowest rank's time."""
+    return ws * units_per_rank / t_max
+
+
 def peak_hbm():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -277,13 +294,7 @@ def run_mtx(args):
     ctx.synchronize()  # raises on any device-side error
     ms = e0.elapsed_time(e1)
     t_local = ms / 1000.0
-    if ws > 1:
-        import torch.distributed as dist
-        tt = torch.tensor([t_local], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
-    else:
-        t_max = t_local
+    t_max = max_over_ranks(t_local, ws)
     counters = [e.counters.cpu().numpy().view(np.uint32) for e in exts]
     for c in counters:
         assert c[4] == 0, f"device status {c[4]}"
@@ -291,8 +302,8 @@ def run_mtx(args):
     T = [int(c[1]) // 3 for c in counters]
     nvox = N ** 3
     steps = args.steps
-    value = ws * 3 * nvox * steps / t_max / 1e9
-    tris_s = ws * sum(T) * steps / t_max
+    value = job_throughput(3 * nvox * steps, ws, t_max) / 1e9
+    tris_s = job_throughput(sum(T) * steps, ws, t_max)
 
     regions = prof.regions()
     prof.close()
@@ -418,13 +429,8 @@ def run_e2e(ctx, vol_dev, ws, steps):
             mm.free()
             L.lib().mtx_volume_free(ctx.handle, C.byref(v))
     torch.cuda.synchronize()
-    t = time.perf_counter() - t0
-    if ws > 1:
-        import torch.distributed as dist
-        tt = torch.tensor([t], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t = float(tt.item())
-    return {"value": ws * 3 * N ** 3 * steps / t / 1e9, "unit": "Gvoxels/s",
+    t = max_over_ranks(time.perf_counter() - t0, ws)
+    return {"value": job_throughput(3 * N ** 3 * steps, ws, t) / 1e9, "unit": "Gvoxels/s",
             "h2d_bytes_per_step": h2d // steps, "d2h_bytes_per_step": d2h // steps, "steps": steps,
             "what": "mtx_volume_upload from pinned host memory -> computeMinMaxMip -> filterActiveBlocks -> "
                     "readActiveBlockCount -> extractMeshletDescriptors -> mesh copied to pinned host memory"}
