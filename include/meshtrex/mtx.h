@@ -297,6 +297,36 @@ mtx_status mtx_extract_plain_async(mtx_context_t ctx, const mtx_volume *vol,
                                    const mtx_push_constants *pc, const mtx_extract_options *opts,
                                    const mtx_mesh_buffers *out);
 
+/* ------------------------------------------------------------ meshlets */
+
+/* Meshlets in the form meshtrex's renderer reads (render.task.glsl:55-250):
+ * each meshlet's triangles index only its own vertices,
+ * [vertexOffset, vertexOffset + vertexCount) of vertexBuffer. */
+typedef struct mtx_meshlet_output {
+    mtx_buffer meshletDescriptorBuffer; /* mtx_meshlet_descriptor per meshlet; indexOffset counts uint32s */
+    mtx_buffer meshletVertexBuffer;     /* uint32 per meshlet vertex: its vertex id in the extraction's mesh */
+    mtx_buffer vertexBuffer;            /* the extraction's vertex records, gathered in meshlet order */
+    mtx_buffer indexBuffer;             /* uint32, 3 per triangle (the mesh's triangle order), ids into vertexBuffer */
+    uint32_t meshletCount;
+    uint32_t vertexCount; /* meshlet vertices: shared vertices appear once per meshlet that uses them */
+    uint32_t indexCount;
+    uint32_t vertexStride; /* bytes, as the extraction's */
+} mtx_meshlet_output;
+
+/* Splits the mesh of an extraction into meshlets of at most maxVertices
+ * (3..64; 64 in meshtrex) vertices and maxPrimitives (1..1024; 126 in
+ * meshtrex) triangles (the limits of marching_cubes_pmb.task.glsl:24-25).
+ * Each block's triangles are taken in their canonical order and a new
+ * meshlet starts when the next triangle's new vertices or the triangle count
+ * would pass a limit, so meshlets never span blocks and the result does not
+ * depend on the run.  Allocates the outputs; free them with
+ * mtx_meshlet_output_free.  meshtrex makes meshlets in its task and mesh
+ * shaders and splits them again in the renderer; this is the same contract as
+ * a post-pass. */
+mtx_status mtx_build_meshlets(mtx_context_t ctx, const mtx_extraction_output *ext, uint32_t maxVertices,
+                              uint32_t maxPrimitives, mtx_meshlet_output *out);
+mtx_status mtx_meshlet_output_free(mtx_context_t ctx, mtx_meshlet_output *out);
+
 /* ------------------------------------------------------------ export */
 
 /* readDataChunkFromBuffer / readCounterFromBuffer

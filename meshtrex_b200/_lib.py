@@ -89,6 +89,12 @@ class MeshBuffers(C.Structure):
                 ("counters", C.c_void_p), ("maxActiveBlocks", C.c_uint64)]
 
 
+class MeshletOutput(C.Structure):
+    _fields_ = [("meshletDescriptorBuffer", Buffer), ("meshletVertexBuffer", Buffer), ("vertexBuffer", Buffer),
+                ("indexBuffer", Buffer), ("meshletCount", C.c_uint32), ("vertexCount", C.c_uint32),
+                ("indexCount", C.c_uint32), ("vertexStride", C.c_uint32)]
+
+
 class BatchJob(C.Structure):
     _fields_ = [("volume", C.c_uint32), ("isovalue", C.c_float)]
 
@@ -166,6 +172,8 @@ SIGNATURES = [
                                               C.POINTER(PushConstants), C.POINTER(ExtractOptions),
                                               _P, C.POINTER(ExtractionOutput)]),
     ("mtx_extraction_free", _ST, [_P, C.POINTER(ExtractionOutput)]),
+    ("mtx_build_meshlets", _ST, [_P, C.POINTER(ExtractionOutput), C.c_uint32, C.c_uint32, C.POINTER(MeshletOutput)]),
+    ("mtx_meshlet_output_free", _ST, [_P, C.POINTER(MeshletOutput)]),
     ("mtx_extract_plain_async", _ST, [_P, C.POINTER(Volume), C.POINTER(PushConstants),
                                       C.POINTER(ExtractOptions), C.POINTER(MeshBuffers)]),
     ("mtx_extract_backward", _ST, [_P, C.POINTER(Volume), C.POINTER(PushConstants), C.POINTER(FilteringOutput),

@@ -313,6 +313,28 @@ def extract_backward(ctx: Context, volume: L.Volume, pc: L.PushConstants, f: Fil
 
 
 @dataclass
+class Meshlets:
+    descriptors: torch.Tensor      # int32 [M, 4] {vertexOffset, indexOffset, vertexCount, primitiveCount}
+    vertex_ids: torch.Tensor       # int32 [MV]: mesh vertex id of each meshlet vertex
+    vertices: torch.Tensor         # float32 [MV, 3|8]: the mesh's vertex records in meshlet order
+    indices: torch.Tensor          # int32 [T, 3]: ids into vertices
+
+
+def build_meshlets(ctx: Context, x: Extraction, max_vertices: int = 64, max_primitives: int = 126) -> Meshlets:
+    """mtx_build_meshlets on a drop-in extraction; copies the results out."""
+    o = L.MeshletOutput()
+    L.check(L.lib().mtx_build_meshlets(ctx.handle, C.byref(x.out), max_vertices, max_primitives, C.byref(o)),
+            "mtx_build_meshlets", ctx.handle)
+    w = max(o.vertexStride // 4, 1)
+    m = Meshlets(device_view(o.meshletDescriptorBuffer.ptr, (o.meshletCount, 4), torch.int32).clone(),
+                 device_view(o.meshletVertexBuffer.ptr, (o.vertexCount,), torch.int32).clone(),
+                 device_view(o.vertexBuffer.ptr, (o.vertexCount, w), torch.float32).clone(),
+                 device_view(o.indexBuffer.ptr, (o.indexCount // 3, 3), torch.int32).clone())
+    L.lib().mtx_meshlet_output_free(ctx.handle, C.byref(o))
+    return m
+
+
+@dataclass
 class Mesh:
     vertices: torch.Tensor   # float32 [V, 3] or [V, 8]
     indices: torch.Tensor    # int32 [T, 3] (uint32 bit pattern)

@@ -280,6 +280,23 @@ mtx_status launch_count(mtx_context *c, const Problem &p, const ExtractArgs &a, 
     return MTX_OK;
 }
 
+// The descriptor scan on its own: vertexOffset / indexOffset of count
+// descriptors from their vertexCount / primitiveCount (totals as launch_count).
+mtx_status launch_desc_scan(mtx_context *c, mtx_meshlet_descriptor *desc, const uint32_t *count, uint64_t capacity,
+                            uint32_t *totals, cudaStream_t s) {
+    const uint32_t ntiles = (uint32_t)std::max<uint64_t>(1, (capacity + kScanTile - 1) / kScanTile);
+    mtx_status r = scratch_reserve(c, c->count_status, sizeof(uint64_t) * (size_t)ntiles);
+    if (r != MTX_OK) return r;
+    MTX_CUDA(c, cudaMemsetAsync(&c->ctrl->count_ticket, 0, sizeof(uint32_t), s));
+    MTX_CUDA(c, cudaMemsetAsync(totals, 0, 4 * sizeof(uint32_t), s));
+    MTX_CUDA(c, cudaMemsetAsync(c->count_status.ptr, 0, sizeof(uint64_t) * ntiles, s));
+    pmb_scan_kernel<<<ntiles, kScanThreads, 0, s>>>(desc, count, (uint64_t *)c->count_status.ptr,
+                                                    &c->ctrl->count_ticket, totals, &c->ctrl->status);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(c, e, "scan launch");
+    return MTX_OK;
+}
+
 // Vertices (when a.vertices is set) and triangles.
 mtx_status launch_emit(mtx_context *c, const Problem &p, const ExtractArgs &a, cudaStream_t s) {
     return launch_stage<true>(c, p, a, s);

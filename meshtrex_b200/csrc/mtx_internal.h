@@ -142,6 +142,9 @@ struct ExtractArgs {
     uint32_t vertex_format, frame, normals, staging, threads;
 };
 mtx_status launch_count(mtx_context *c, const Problem &p, const ExtractArgs &a, cudaStream_t s);
+// The descriptor scan alone over *count descriptors (capacity bounds them).
+mtx_status launch_desc_scan(mtx_context *c, mtx_meshlet_descriptor *desc, const uint32_t *count, uint64_t capacity,
+                            uint32_t *totals, cudaStream_t s);
 mtx_status launch_emit(mtx_context *c, const Problem &p, const ExtractArgs &a, cudaStream_t s);
 
 // Whether the volume can be staged with TMA (row pitch and base 16-byte aligned).

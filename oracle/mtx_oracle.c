@@ -555,3 +555,66 @@ int orc_pipeline(const orc_volume *v, const uint32_t blk[3], float iso, int nthr
     free(ids);
     return rc;
 }
+
+/* Meshlet split (see the header): a straight restatement with a linear
+ * search of the current meshlet's vertex list. */
+uint64_t orc_meshlets(const uint32_t *ntri_per_block, uint32_t n_blocks, const uint32_t *indices, uint32_t max_v,
+                      uint32_t max_p, uint32_t *desc, uint32_t *mverts, uint32_t *midx, uint64_t *n_mverts) {
+    uint64_t m = 0, mv = 0, t = 0;
+    uint32_t list[1024];
+    for (uint32_t b = 0; b < n_blocks; ++b) {
+        const uint64_t t1 = t + ntri_per_block[b];
+        uint32_t cur_v = 0, cur_p = 0;
+        uint64_t first_t = t, vstart = mv;
+        for (; t < t1; ++t) {
+            uint32_t loc[3], fresh = 0;
+            for (int k = 0; k < 3; ++k) {
+                loc[k] = UINT32_MAX;
+                for (uint32_t i = 0; i < cur_v; ++i)
+                    if (list[i] == indices[3 * t + k]) loc[k] = i;
+                int dup = 0;
+                for (int j = 0; j < k; ++j) dup |= indices[3 * t + j] == indices[3 * t + k];
+                if (loc[k] == UINT32_MAX && !dup) ++fresh;
+            }
+            if (cur_p > 0 && (cur_v + fresh > max_v || cur_p >= max_p)) {
+                if (desc) {
+                    desc[4 * m + 0] = (uint32_t)vstart;
+                    desc[4 * m + 1] = (uint32_t)(3 * first_t);
+                    desc[4 * m + 2] = cur_v;
+                    desc[4 * m + 3] = cur_p;
+                }
+                ++m;
+                vstart = mv;
+                cur_v = cur_p = 0;
+                first_t = t;
+                loc[0] = loc[1] = loc[2] = UINT32_MAX;
+            }
+            for (int k = 0; k < 3; ++k) {
+                const uint32_t id = indices[3 * t + k];
+                if (loc[k] == UINT32_MAX) {
+                    for (uint32_t i = 0; i < cur_v; ++i)
+                        if (list[i] == id) loc[k] = i;
+                }
+                if (loc[k] == UINT32_MAX) {
+                    loc[k] = cur_v;
+                    list[cur_v++] = id;
+                    if (mverts) mverts[mv] = id;
+                    ++mv;
+                }
+                if (midx) midx[3 * t + k] = (uint32_t)(vstart + loc[k]);
+            }
+            ++cur_p;
+        }
+        if (cur_p > 0) {
+            if (desc) {
+                desc[4 * m + 0] = (uint32_t)vstart;
+                desc[4 * m + 1] = (uint32_t)(3 * first_t);
+                desc[4 * m + 2] = cur_v;
+                desc[4 * m + 3] = cur_p;
+            }
+            ++m;
+        }
+    }
+    if (n_mverts) *n_mverts = mv;
+    return m;
+}

@@ -98,6 +98,20 @@ int orc_mc_extract(const orc_volume *v, const uint32_t blk[3], float iso, const 
 int orc_mc_adjoint(const orc_volume *v, const uint32_t blk[3], float iso, const uint32_t *ids,
                    uint32_t n_active, const float *dl_dxyz, double *dl_dfield, double *dl_diso);
 
+/* Meshlet split of a canonical mesh (the rule of mtx_build_meshlets; no
+ * meshtrex counterpart restated here, its limits are those of
+ * marching_cubes_pmb.task.glsl:24-25): each block's triangles in order; a
+ * triangle starts a new meshlet when its vertices not yet in the current
+ * meshlet would take it past max_v, or the meshlet already has max_p
+ * triangles.  A meshlet's vertices are listed in the order its triangles
+ * first use them.  Writes per meshlet {vertexOffset, indexOffset, vertexCount,
+ * primitiveCount} (desc, 4 words), the mesh vertex id of every meshlet vertex
+ * (mverts) and the indices into the meshlet vertex stream (midx, 3 per
+ * triangle); NULL outputs count only.  Returns the number of meshlets and
+ * sets *n_mverts. */
+uint64_t orc_meshlets(const uint32_t *ntri_per_block, uint32_t n_blocks, const uint32_t *indices, uint32_t max_v,
+                      uint32_t max_p, uint32_t *desc, uint32_t *mverts, uint32_t *midx, uint64_t *n_mverts);
+
 /* Whole plain pipeline (min/max -> compaction -> extraction) in one call, for
  * the CPU baseline: counts only when the output pointers are NULL. */
 int orc_pipeline(const orc_volume *v, const uint32_t blk[3], float iso, int nthreads,

@@ -71,6 +71,8 @@ def lib():
         L.orc_pipeline.argtypes = [C.POINTER(_Vol), U32P, F, C.c_int, C.POINTER(_Counts),
                                    U32P, P, P]
         L.orc_pipeline.restype = C.c_int
+        L.orc_meshlets.argtypes = [P, C.c_uint32, P, C.c_uint32, C.c_uint32, P, P, P, C.POINTER(U64)]
+        L.orc_meshlets.restype = U64
         L.orc_key_of_f32.argtypes = [F]
         L.orc_key_of_f32.restype = C.c_uint32
         L.orc_f32_of_key.argtypes = [C.c_uint32]
@@ -222,6 +224,20 @@ def mc_extract(v: np.ndarray, block, iso: float, ids: np.ndarray, frame: int = F
         if rc != 0:
             raise RuntimeError(f"oracle extract failed ({rc})")
     return Mesh(ids, nv[:n], nt[:n], xyz, xyz64, nrm, idx)
+
+
+def meshlets(ntri_per_block: np.ndarray, indices: np.ndarray, max_v: int = 64, max_p: int = 126):
+    """(descriptors uint32 [M, 4], meshlet vertex ids [MV], indices into them [T, 3])."""
+    nt = np.ascontiguousarray(ntri_per_block, np.uint32)
+    idx = np.ascontiguousarray(indices, np.uint32).reshape(-1)
+    mv = C.c_uint64(0)
+    m = lib().orc_meshlets(nt.ctypes.data, len(nt), idx.ctypes.data, max_v, max_p, None, None, None, C.byref(mv))
+    desc = np.zeros((m, 4), np.uint32)
+    mverts = np.zeros(mv.value, np.uint32)
+    midx = np.zeros(idx.size, np.uint32)
+    lib().orc_meshlets(nt.ctypes.data, len(nt), idx.ctypes.data, max_v, max_p, desc.ctypes.data,
+                       mverts.ctypes.data, midx.ctypes.data, C.byref(mv))
+    return desc, mverts, midx.reshape(-1, 3)
 
 
 def mc_adjoint(v: np.ndarray, block, iso: float, ids: np.ndarray, dl_dxyz: np.ndarray):

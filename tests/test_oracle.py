@@ -192,3 +192,17 @@ def test_adjoint_matches_finite_differences(oracle):
         assert abs(fd - dfield[tuple(zyx)]) <= 1e-4 * max(abs(fd), 1e-3)
     lp, lm = _fp64_loss(f - h, 4, iso, ids), _fp64_loss(f + h, 4, iso, ids)  # iso + h <=> field - h
     assert abs((lp - lm) / (2 * h) - diso) <= 1e-4 * max(abs(diso), 1e-3)
+
+
+def test_meshlet_rule_on_a_hand_mesh(oracle):
+    # block 0: two triangles share an edge (4 vertices fit a 4-vertex meshlet),
+    # the third needs 3 more vertices and starts a new meshlet; block 1's
+    # triangles start their own meshlet and reuse vertex 0 as a new copy
+    nt = np.array([3, 2], np.uint32)
+    idx = np.array([[0, 1, 2], [1, 2, 3], [4, 5, 6], [7, 8, 9], [8, 9, 0]], np.uint32)
+    d, mv, mi = oracle.meshlets(nt, idx, 4, 126)
+    np.testing.assert_array_equal(d, [[0, 0, 4, 2], [4, 6, 3, 1], [7, 9, 4, 2]])
+    np.testing.assert_array_equal(mv, [0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 0])
+    np.testing.assert_array_equal(mv[mi], idx)
+    d2, _, _ = oracle.meshlets(nt, idx, 64, 1)  # one triangle per meshlet
+    assert len(d2) == 5 and (d2[:, 3] == 1).all()
