@@ -19,7 +19,7 @@
 
 namespace mtx {
 
-constexpr uint32_t kRing = 192;  // queued jobs: at most 31 left + 32 cells x 5 triangles
+constexpr uint32_t kRing = 256;  // queued jobs (a power of two): at most 31 left + 32 cells x 5 triangles
 
 // Single float tile, vertex table in its place, list, ring.
 __host__ __device__ inline WPlan make_wplan_balanced(uint32_t B) {
@@ -225,7 +225,7 @@ __device__ __forceinline__ uint32_t table_vertex(uint32_t c, uint32_t e, const u
 
 // ---------------------------------------------------------- resolution
 // Vertex jobs [done, done + n), n <= 32, one per lane: job = tile index of
-// the owner voxel | axis << 13, at jobs[i % kRing].
+// the owner voxel | axis << 13, at jobs[i & (kRing - 1)].
 template <bool GENERIC>
 __device__ __forceinline__ void resolve_vertices(const Problem &p, const WPlan &pl, unsigned char *ws, const Geo &g,
                                                  uint32_t done, uint32_t n, uint32_t vbase, void *vertices,
@@ -236,7 +236,7 @@ __device__ __forceinline__ void resolve_vertices(const Problem &p, const WPlan &
     const uint32_t *jobs = reinterpret_cast<const uint32_t *>(ws + pl.off_jobs);
     const bool xyz = !GENERIC || vfmt == MTX_VERTEX_XYZ;
     if (lane < n) {
-        const uint32_t job = jobs[(done + lane) % kRing];
+        const uint32_t job = jobs[(done + lane) & (kRing - 1)];
         const uint32_t t3 = job & 0x1fffu, a = job >> 13;
         const uint32_t iq = fdiv(t3, pl.rB1);
         const uint32_t x = t3 - iq * B1, z = fdiv(iq, pl.rB1), y = iq - z * B1;
@@ -273,7 +273,7 @@ __device__ __forceinline__ void resolve_triangles(const WPlan &pl, unsigned char
     uint32_t *stage = reinterpret_cast<uint32_t *>(ws + pl.off_stage);
     const uint32_t *jobs = reinterpret_cast<const uint32_t *>(ws + pl.off_jobs);
     if (lane < n) {
-        const uint32_t job = jobs[(done + lane) % kRing];
+        const uint32_t job = jobs[(done + lane) & (kRing - 1)];
         const uint32_t cell = job & 0x1fffu, t = (job >> 13) & 7u;
         const uint64_t w = tab[job >> 16] >> (4 + 12 * t);
         stage[3 * lane + 0] = table_vertex(cell, (uint32_t)(w & 0xFu), owner, B1, vtab, vmsk, bad);
@@ -329,7 +329,7 @@ __device__ __forceinline__ void emit_block_balanced(const Problem &p, const WPla
             uint32_t tot;
             uint32_t j = top + warp_excl_scan(__popc(m), tot);
             for (uint32_t a = 0; a < 3; ++a)
-                if ((m >> a) & 1u) jobs[(j++) % kRing] = ti | (a << 13);
+                if ((m >> a) & 1u) jobs[(j++) & (kRing - 1)] = ti | (a << 13);
             top += tot;
             __syncwarp();
             const bool last = v0 + 32 >= nc;
@@ -358,7 +358,7 @@ __device__ __forceinline__ void emit_block_balanced(const Problem &p, const WPla
         }
         uint32_t tot;
         const uint32_t j = top + warp_excl_scan(n, tot);
-        for (uint32_t t = 0; t < n; ++t) jobs[(j + t) % kRing] = ti | (t << 13) | (cfg << 16);
+        for (uint32_t t = 0; t < n; ++t) jobs[(j + t) & (kRing - 1)] = ti | (t << 13) | (cfg << 16);
         top += tot;
         __syncwarp();
         const bool last = c0 + 32 >= nmix;
