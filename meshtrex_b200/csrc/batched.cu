@@ -466,13 +466,17 @@ __device__ __forceinline__ void batch_emit_block(const BatchArgs &a, const Probl
     const mtx_meshlet_descriptor d{q.x, q.y, q.z, q.w};
     const uint32_t nb_rk = neighbour_rank<false>(p, g, id, a.rank_pool + rank_off);
     const uint32_t nb_vb = nb_rk != kNoVertex ? __ldcg(&a.desc[nb_rk].vertexOffset) : kNoVertex;
+    tile_load_float(p, pl, reinterpret_cast<float *>(ws + pl.off_tile[0]), g);
+    void *verts = a.vertices ? (void *)((char *)a.vertices + jr.vertexOffset * a.vsz) : nullptr;
+    if (!emit_vertices_balanced<GENERIC>(p, pl, ws, g, d, ntab, jr.indexCount / 3u, verts, jr.vertexCount, a.vfmt,
+                                         a.frame, a.normals, &a.ctrl->status, r))
+        return;
+    // the tile is dead: the vertex table takes its place, its context layer
+    // gathered from the neighbours' face records
     uint32_t rec[CPL];
     gather_issue<CPL, false>(p, pl, g, nb_rk, a.faces, a.face_stride, rec);
-    tile_load_float(p, pl, reinterpret_cast<float *>(ws + pl.off_tile[0]), g);
-    gather_finish<CPL>(pl, nb_vb, rec, ws);
-    void *verts = a.vertices ? (void *)((char *)a.vertices + jr.vertexOffset * a.vsz) : nullptr;
-    emit_block_balanced<GENERIC>(p, pl, ws, g, d, tab, ntab, owner, a.indices + jr.indexOffset, jr.indexCount / 3u,
-                                 verts, jr.vertexCount, a.vfmt, a.frame, a.normals, &a.ctrl->status, r);
+    fill_context_vertices<CPL>(pl, ws, nb_vb, rec);
+    emit_triangles_balanced(p, pl, ws, g, d, tab, ntab, owner, a.indices + jr.indexOffset, &a.ctrl->status, r);
 }
 
 // ------------------------------------------------------------ the kernel
@@ -624,10 +628,9 @@ WPlan plan_in_layout(uint32_t B, const WPlan &L) {
     p.off_cross = L.off_cross;
     p.off_vp = L.off_vp;
     p.off_list = L.off_list;
-    p.off_nvid = L.off_nvid;
-    p.off_nm = L.off_nm;
     p.off_vmsk = L.off_vmsk;
     p.off_stage = L.off_stage;
+    p.off_tstage = L.off_tstage;
     p.off_jobs = L.off_jobs;
     p.bytes = L.bytes;
     return p;
@@ -834,6 +837,10 @@ mtx_status mtx_batch_create(mtx_context_t c, const mtx_batch_desc *d, mtx_batch_
     b->smem = kTableBytes + a.block_warps * L.bytes;
     KernelFn fn = batch_kernel(b->variant);
     e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->smem);
+    // all of the unified L1 as shared memory: more resident warps hide the
+    // block bodies' shared-memory latencies
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(fn, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
     int occ = 0;
     if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kBThreads, b->smem);
     if (e != cudaSuccess) {

@@ -10,9 +10,13 @@
 // vertex id and owned-edge mask of every voxel of the (B+1)^3 tile.
 //
 // Layout (make_wplan_balanced): a single float tile, which the vertex table
-// takes over once the block's vertices are written; the neighbours' face
-// records wait in compact arrays until then.  Same output as the row bodies,
-// bit for bit.
+// takes over once the block's vertices are written; the context layer of the
+// table is gathered from the neighbours' face records at that point.  The
+// staging of 32 vertices lives in the owned-edge masks (written after the
+// vertices), that of 32 triangles in the crossing rows (dead once the table
+// is filled), and the row prefixes in the job ring (dead until the first job
+// is queued), so that four CTAs of eight warps fit an SM at B = 8.  Same
+// output as the row bodies, bit for bit.
 #pragma once
 
 #include "pmb_device.cuh"
@@ -21,7 +25,6 @@ namespace mtx {
 
 constexpr uint32_t kRing = 256;  // queued jobs (a power of two): at most 31 left + 32 cells x 5 triangles
 
-// Single float tile, vertex table in its place, list, ring.
 __host__ __device__ inline WPlan make_wplan_balanced(uint32_t B) {
     WPlan p{};
     p.B = B;
@@ -33,35 +36,30 @@ __host__ __device__ inline WPlan make_wplan_balanced(uint32_t B) {
     p.rBB = (uint32_t)((0x100000000ull + B * B - 1) / (B * B));
     p.R = 32 / B;
     p.PX = B + 1;
-    const uint32_t T3 = p.B1 * p.B1 * p.B1;
+    const uint32_t T3 = p.B1 * p.B1 * p.B1, stage = 4 * kStageWords;
     p.tile_bytes = 4 * T3;
     p.nbuf = 1;
     uint32_t o = 0;
     p.off_tile[0] = p.off_tile[1] = o;
     p.off_vtab = o;  // the vertex table replaces the tile (same size)
-    o = align_up(o + p.tile_bytes, 128);
-    p.off_bar = o;
-    o += 16;
+    o = align_up(o + p.tile_bytes, 16);
+    p.off_bar = 0;   // unused: tiles are staged by plain loads
     p.off_rows = o;
     o = align_up(o + 4 * p.B1 * p.B1, 16);
     p.off_cross = o;
     o = align_up(o + 12 * p.BB, 16);
-    p.off_vp = o;
-    o = align_up(o + 4 * p.BB, 16);
     p.off_list = o;  // uint16 cell or voxel indices, canonical order
     o = align_up(o + 2 * B * B * B, 16);
-    p.off_nvid = o;  // context layer's first vertex ids, compact order (ctx_voxel)
-    o = align_up(o + 4 * p.nb3, 16);
-    p.off_nm = o;
-    o = align_up(o + p.nb3, 16);
     p.off_vmsk = o;
     o = align_up(o + T3, 16);
-    p.off_stage = o;
-    o = align_up(o + 4 * kStageWords, 16);
     p.off_jobs = o;
     o = align_up(o + 4 * kRing, 16);
-    p.off_tp = 0;
-    p.bytes = align_up(o, 128);
+    p.off_vp = p.off_jobs;  // 4 * BB <= 4 * kRing for B <= 16
+    p.off_stage = T3 >= stage ? p.off_vmsk : o;
+    p.off_tstage = 12 * p.BB >= stage ? p.off_cross : o;
+    if (T3 < stage || 12 * p.BB < stage) o = align_up(o + stage, 16);
+    p.off_nvid = p.off_nm = p.off_tp = 0;  // unused
+    p.bytes = o;
     return p;
 }
 
@@ -173,35 +171,53 @@ __device__ __forceinline__ void count_block_balanced(const Problem &p, const WPl
 }
 
 // ---------------------------------------------------------- vertex table
-// The context layer's entries, from the compact arrays gather_finish filled.
-__device__ __forceinline__ void fill_context_vertices(const WPlan &pl, unsigned char *ws) {
-    const uint32_t lane = threadIdx.x & 31, B1 = pl.B1;
-    const uint32_t *nvid = reinterpret_cast<const uint32_t *>(ws + pl.off_nvid);
-    const uint8_t *nm = ws + pl.off_nm;
+// The context layer's entries (some coordinate == B), straight from the
+// gathered face records (gather_issue; nb_vb: lane c holds neighbour c's
+// first vertex id).
+template <int CPL>
+__device__ __forceinline__ void fill_context_vertices(const WPlan &pl, unsigned char *ws, uint32_t nb_vb,
+                                                      const uint32_t rec[CPL]) {
+    const uint32_t lane = threadIdx.x & 31, B = pl.B, B1 = pl.B1, nb3 = pl.nb3;
     uint32_t *vtab = reinterpret_cast<uint32_t *>(ws + pl.off_vtab);
     uint8_t *vmsk = ws + pl.off_vmsk;
-    for (uint32_t j = lane; j < pl.nb3; j += 32) {
+#pragma unroll
+    for (uint32_t k = 0; k < CPL; ++k) {
+        if (k * 32 >= nb3) continue;  // warp-uniform
+        const uint32_t j = k * 32 + lane;
         uint32_t x, y, z;
-        ctx_voxel(pl, j, x, y, z);
-        const uint32_t i = (z * B1 + y) * B1 + x;
-        vtab[i] = nvid[j];
-        vmsk[i] = nm[j];
+        ctx_voxel(pl, j < nb3 ? j : 0, x, y, z);
+        const uint32_t c = j < nb3 ? ((x == B) | ((y == B) << 1) | ((z == B) << 2)) : 1u;
+        const uint32_t vb = __shfl_sync(0xffffffffu, nb_vb, c);
+        if (j < nb3) {
+            const bool present = rec[k] >> 31;
+            const uint32_t i = (z * B1 + y) * B1 + x;
+            vtab[i] = present ? vb + (rec[k] & 0xffffffu) : kNoVertex;
+            vmsk[i] = present ? (uint8_t)((rec[k] >> 24) & 7u) : (uint8_t)0;
+        }
     }
 }
 
-// The block's own voxels, from the crossing rows and the row prefixes.
+// The block's own voxels, from the crossing rows.  Lane l owns rows
+// [l*R, l*R + R), as in block_counts, so one warp scan of the rows' vertex
+// counts gives every row its first vertex.
 __device__ __forceinline__ void fill_own_vertices(const WPlan &pl, unsigned char *ws, uint32_t vbase) {
     const uint32_t lane = threadIdx.x & 31, B = pl.B, BB = pl.BB, B1 = pl.B1, R = (BB + 31) / 32;
     const uint32_t *cross = reinterpret_cast<const uint32_t *>(ws + pl.off_cross);
-    const uint32_t *vp = reinterpret_cast<const uint32_t *>(ws + pl.off_vp);
     uint32_t *vtab = reinterpret_cast<uint32_t *>(ws + pl.off_vtab);
     uint8_t *vmsk = ws + pl.off_vmsk;
+    uint32_t cnt = 0;
+    for (uint32_t k = 0; k < R; ++k) {
+        const uint32_t q = lane * R + k;
+        if (q >= BB) break;
+        cnt += __popc(cross[q]) + __popc(cross[BB + q]) + __popc(cross[2 * BB + q]);
+    }
+    uint32_t tot;
+    uint32_t run = vbase + warp_excl_scan(cnt, tot);
     for (uint32_t k = 0; k < R; ++k) {
         const uint32_t q = lane * R + k;
         if (q >= BB) break;
         const uint32_t z = fdiv(q, pl.rB), y = q - z * B, row = (z * B1 + y) * B1;
         const uint32_t xc = cross[q], yc = cross[BB + q], zc = cross[2 * BB + q];
-        uint32_t run = vbase + vp[q];
         for (uint32_t x = 0; x < B; ++x) {
             const uint32_t m = ((xc >> x) & 1u) | (((yc >> x) & 1u) << 1) | (((zc >> x) & 1u) << 2);
             vmsk[row + x] = (uint8_t)m;
@@ -209,6 +225,7 @@ __device__ __forceinline__ void fill_own_vertices(const WPlan &pl, unsigned char
             run += __popc(m);
         }
     }
+    __syncwarp();
 }
 
 // Vertex id of cube edge e of the cell at tile index c: the owner voxel
@@ -270,7 +287,7 @@ __device__ __forceinline__ void resolve_triangles(const WPlan &pl, unsigned char
     const uint32_t lane = threadIdx.x & 31, B1 = pl.B1;
     const uint32_t *vtab = reinterpret_cast<const uint32_t *>(ws + pl.off_vtab);
     const uint8_t *vmsk = ws + pl.off_vmsk;
-    uint32_t *stage = reinterpret_cast<uint32_t *>(ws + pl.off_stage);
+    uint32_t *stage = reinterpret_cast<uint32_t *>(ws + pl.off_tstage);
     const uint32_t *jobs = reinterpret_cast<const uint32_t *>(ws + pl.off_jobs);
     if (lane < n) {
         const uint32_t job = jobs[(done + lane) & (kRing - 1)];
@@ -286,26 +303,26 @@ __device__ __forceinline__ void resolve_triangles(const WPlan &pl, unsigned char
 }
 
 // ---------------------------------------------------------- emit body
-// Emit body (emit_block) for a block whose float tile is staged and whose
-// context layer has been gathered into the compact arrays.
+// First half of the emit body (emit_block) for a block whose float tile is
+// staged: checks the capacities, writes the block's vertices and returns
+// whether its triangles are still to be written (emit_triangles_balanced,
+// after the caller has put the context layer into the vertex table).
 template <bool GENERIC>
-__device__ __forceinline__ void emit_block_balanced(const Problem &p, const WPlan &pl, unsigned char *ws,
-                                                    const Geo &g, const mtx_meshlet_descriptor &d,
-                                                    const uint64_t *tab, const uint8_t *ntab, const uint8_t *owner,
-                                                    uint32_t *indices, uint64_t tcap, void *vertices, uint64_t vcap,
-                                                    uint32_t vfmt, uint32_t frame, uint32_t normals, DevStatus *st,
-                                                    uint32_t r) {
+__device__ __forceinline__ bool emit_vertices_balanced(const Problem &p, const WPlan &pl, unsigned char *ws,
+                                                       const Geo &g, const mtx_meshlet_descriptor &d,
+                                                       const uint8_t *ntab, uint64_t tcap, void *vertices,
+                                                       uint64_t vcap, uint32_t vfmt, uint32_t frame,
+                                                       uint32_t normals, DevStatus *st, uint32_t r) {
     const uint32_t lane = threadIdx.x & 31, B = pl.B, BB = pl.BB, B1 = pl.B1;
-    const uint32_t *rows = reinterpret_cast<const uint32_t *>(ws + pl.off_rows);
     const uint32_t *cross = reinterpret_cast<const uint32_t *>(ws + pl.off_cross);
     const uint16_t *list = reinterpret_cast<const uint16_t *>(ws + pl.off_list);
     uint32_t *jobs = reinterpret_cast<uint32_t *>(ws + pl.off_jobs);
     const uint32_t tbase = d.indexOffset / 3u;
     if ((uint64_t)tbase + d.primitiveCount > tcap || (vertices && (uint64_t)d.vertexOffset + d.vertexCount > vcap)) {
         if (lane == 0) report(st, MTX_ERR_CAPACITY, kSiteEmitCapacity, r, 2);
-        return;
+        return false;
     }
-    if (!(d.primitiveCount || (vertices && d.vertexCount))) return;
+    if (!(d.primitiveCount || (vertices && d.vertexCount))) return false;
     build_rows<float>(p, pl, ws, 0, g);
     uint32_t bnv, bnt;
     block_counts_balanced(p, pl, ws, g, ntab, false, bnv, bnt);
@@ -340,9 +357,21 @@ __device__ __forceinline__ void emit_block_balanced(const Problem &p, const WPla
             }
         }
     }
-    if (!d.primitiveCount) return;
-    // the tile is dead from here on: the vertex table takes its place
-    fill_context_vertices(pl, ws);
+    return d.primitiveCount != 0;
+}
+
+// Second half: the block's own voxels into the vertex table, then its
+// triangles.
+__device__ __forceinline__ void emit_triangles_balanced(const Problem &p, const WPlan &pl, unsigned char *ws,
+                                                        const Geo &g, const mtx_meshlet_descriptor &d,
+                                                        const uint64_t *tab, const uint8_t *ntab,
+                                                        const uint8_t *owner, uint32_t *indices, DevStatus *st,
+                                                        uint32_t r) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t *rows = reinterpret_cast<const uint32_t *>(ws + pl.off_rows);
+    const uint16_t *list = reinterpret_cast<const uint16_t *>(ws + pl.off_list);
+    uint32_t *jobs = reinterpret_cast<uint32_t *>(ws + pl.off_jobs);
+    const uint32_t tbase = d.indexOffset / 3u;
     fill_own_vertices(pl, ws, d.vertexOffset);
     // triangles: the mixed cells 32 at a time; a warp scan of their triangle
     // counts queues the jobs (tile index | t << 13 | case << 16) in the ring

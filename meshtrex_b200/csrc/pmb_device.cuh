@@ -47,7 +47,7 @@ struct WPlan {
     uint32_t rB, rB1, rBB;  // ceil(2^32 / d) reciprocals: n / d == __umulhi(n, r) for the sizes used here
     uint32_t R;             // block rows walked per round of 32 lanes (32 / B)
     uint32_t off_tile[2], off_bar, off_rows, off_cross, off_vp, off_tp, off_nvid, off_nm, off_stage, off_jobs;
-    uint32_t off_vtab, off_vmsk, off_list;  // balanced bodies only (pmb_balanced.cuh)
+    uint32_t off_vtab, off_vmsk, off_list, off_tstage;  // balanced bodies only (pmb_balanced.cuh)
     uint32_t bytes;       // per warp
     uint32_t tile_bytes;  // one tile (the TMA transaction size)
 };
