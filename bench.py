@@ -366,7 +366,7 @@ def run_mtx(args):
                        "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
             "tris_per_s": tris_s, "vertices_per_step": sum(V), "triangles_per_step": sum(T),
             "stages_ms_per_extraction": per_stage,
-            "roofline": {"bound": "hbm", "kernel": "minmax_leaf_vec_kernel<uint16_t,8>",
+            "roofline": {"bound": "hbm", "kernel": "minmax_leaf_tma_kernel<uint16_t,8>",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": (achieved / peak) if achieved else None,
                          "traffic": traffic, "algorithmic_bytes": leaf_bytes, "peak_kind": f"{peak_kind} (burst copy)"},

@@ -476,7 +476,8 @@ mtx_status mtx_profiler_region(mtx_profiler_t prof, uint32_t i, char name[64], d
  * workgroup sizes and specialization constants (extractionPipeline.cpp:238-256). */
 typedef struct mtx_tuning {
     uint32_t minmaxZChunk;  /* block slabs per warp in the min/max pass */
-    uint32_t minmaxSlices;  /* z slices whose loads are issued together: 1, 2 (default) or 4 */
+    uint32_t minmaxSlices;  /* 0 (default): a TMA ring of z slices for 2- and 4-byte voxels (else 2);
+                               1, 2 or 4: the load-based pass with that many z slices in flight */
     uint32_t extractWarps;  /* warps per CTA of the extraction passes: 1, 2, 4 (default) or 8 */
     uint32_t staging;       /* mtx_staging used when the extract options say AUTO */
 } mtx_tuning;
@@ -498,7 +499,7 @@ typedef struct mtx_autotune_result {
 #define MTX_AUTOTUNE_QUICK 2u        /* one repetition per candidate instead of the best of three */
 
 /* Picks the block edge (4, 8, 16), the warps per CTA of the extraction passes
- * (2, 4, 8), the staging (TMA or plain loads) and the min/max slices (1, 2, 4)
+ * (2, 4, 8), the staging (TMA or plain loads) and the min/max pass (TMA ring or 1, 2, 4 slices of loads)
  * for one volume by timing the whole plain extraction of each candidate at
  * `isovalue` on the device.  The score is the sum of the stage times that CUDA
  * events record.  The choice is cached per (dims, dtype, device name) in the

@@ -129,6 +129,11 @@ void mip_layout(const uint32_t g[3], int levels, uint32_t ext[][3], uint64_t *of
 
 // ------------------------------------------------------------ tensor maps
 mtx_status make_volume_tensor_map(mtx_context *c, const Problem &p, uint32_t box_x, CUtensorMap *map) {
+    return make_volume_tensor_map_box(c, p, box_x, p.B + 1, p.B + 1, map);
+}
+
+mtx_status make_volume_tensor_map_box(mtx_context *c, const Problem &p, uint32_t box_x, uint32_t box_y,
+                                      uint32_t box_z, CUtensorMap *map) {
     static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
     static std::once_flag once;
     std::call_once(once, [] {
@@ -145,9 +150,9 @@ mtx_status make_volume_tensor_map(mtx_context *c, const Problem &p, uint32_t box
                                                         : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
     cuuint64_t dims[3] = {p.X, p.Y, p.Z};
     cuuint64_t strides[2] = {(cuuint64_t)p.X * esz, (cuuint64_t)p.X * p.Y * esz};
-    cuuint32_t box[3] = {box_x, p.B + 1, p.B + 1};
+    cuuint32_t box[3] = {box_x, box_y, box_z};
     cuuint32_t estr[3] = {1, 1, 1};
-    if ((uintptr_t)p.vol % 16 || strides[0] % 16 || box_x > 256 || (box_x * esz) % 16)
+    if ((uintptr_t)p.vol % 16 || strides[0] % 16 || box_x > 256 || box_y > 256 || box_z > 256 || (box_x * esz) % 16)
         return fail(c, MTX_ERR_INTERNAL, "volume layout does not allow a TMA tile");
     CUresult r = encode(map, dt, 3, const_cast<void *>(p.vol), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                         CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,

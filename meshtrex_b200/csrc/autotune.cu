@@ -159,8 +159,9 @@ extern "C" mtx_status mtx_autotune(mtx_context_t c, const mtx_volume *vol, float
         }
         if (rs != MTX_OK) break;
     }
-    // stage 2: z slices whose loads the min/max pass issues together, at the chosen shape
-    for (uint32_t slices : {1u, 4u}) {
+    // stage 2: the load-based min/max pass with 1, 2 or 4 z slices in flight
+    // against the default (the TMA ring where the dtype allows it), at the chosen shape
+    for (uint32_t slices : {1u, 2u, 4u}) {
         if (rs != MTX_OK) break;
         c->tuning = best.t;
         c->tuning.minmaxSlices = slices;

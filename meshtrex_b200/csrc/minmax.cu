@@ -23,6 +23,229 @@ __global__ void __launch_bounds__(128) minmax_leaf_vec_kernel(const T *__restric
     minmax_leaf_vec_warp<T, B, ZU>(vol, X, Y, Z, GX, GY, GZ, nXS, zchunk, w, leaf);
 }
 
+// TMA-fed leaf pass for 2- and 4-byte voxels: persistent CTAs of four warps,
+// four per SM.  A work item is (x-strip of 512 bytes, run of ZC block slabs,
+// group of four block rows), taken in that order so that the strips of one row
+// and the items sharing a halo slice or row run side by side (L2 serves the
+// repeats, DRAM sees whole rows).  Per z
+// slice thread 0 issues two TMA boxes into a ring of S stages: the strip's
+// 4B+1 rows and, beyond them, the 16-byte halo column (out-of-volume parts
+// read as zero and are masked).  Warp w folds block row w of the group with
+// the per-lane arithmetic of the load-based body: lane l owns 16 bytes of
+// every row, the +1 column of a block comes from the next lane by shuffle
+// (lane 31: from the halo box), and a slice at z = (bz+1)*B closes block bz
+// and opens bz+1; even and odd rows fold into separate registers so that the
+// dependent chains stay short.  Loads in flight live in shared memory (about
+// 35 KB per CTA), not in registers (40 per thread), so an SM keeps room for
+// the extraction kernels of other streams.
+constexpr int kTmaRows(int B) { return 4 * B + 1; }
+constexpr uint32_t kTmaMain(int B) { return (uint32_t)kTmaRows(B) * 512u; }
+constexpr uint32_t kTmaHalo(int B) { return ((uint32_t)kTmaRows(B) * 16u + 127u) / 128u * 128u; }
+constexpr uint32_t kTmaStage(int B) { return (kTmaMain(B) + 127u) / 128u * 128u + kTmaHalo(B); }
+constexpr int kTmaStages(int B) { return B == 4 ? 4 : 2; }  // about 35 KB per CTA at B = 4 and 8
+constexpr int kTmaCtasPerSm = 4;  // 16 warps: enough to hide the fold's latencies, smem left for other kernels
+
+struct TmaLeafArgs {
+    uint32_t X, Y, Z, GX, GY, GZ;
+    uint32_t nXS, nYG, nZC, zchunk;
+    uint32_t nitems;
+};
+
+template <typename T, int B>
+__global__ void __launch_bounds__(128) minmax_leaf_tma_kernel(const __grid_constant__ CUtensorMap map_main,
+                                                                 const __grid_constant__ CUtensorMap map_halo,
+                                                                 const TmaLeafArgs a, uint2 *__restrict__ leaf,
+                                                                 DevStatus *st) {
+    using L16 = Lane16<T>;
+    constexpr int V = L16::V;
+    constexpr int SEG = 32 * V;
+    constexpr int NB = V >= B ? V / B : 1;   // blocks per lane
+    constexpr int LPB = V >= B ? 1 : B / V;  // lanes per block
+    constexpr int CNT = V >= B ? B : V;      // elements of one block in one lane
+    constexpr int S = kTmaStages(B);
+    constexpr uint32_t MAIN = kTmaMain(B), STAGE = kTmaStage(B);
+    constexpr uint32_t HOFF = (MAIN + 127u) / 128u * 128u;
+    constexpr uint32_t TX = MAIN + (uint32_t)kTmaRows(B) * 16u;  // bytes per stage
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t bars[S];
+    __shared__ uint32_t s_fail;
+    const uint32_t tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+
+    if (tid == 0) {
+        for (int i = 0; i < S; ++i) mbar_init(&bars[i], 1);
+        fence_mbar_init();
+        s_fail = 0;
+        prefetch_tensormap(&map_main);
+        prefetch_tensormap(&map_halo);
+    }
+    __syncthreads();
+
+    // the CTA's slices in order: items blockIdx.x, blockIdx.x + gridDim.x, ...
+    // each from z = bz0*B to min(bz1*B, Z-1)
+    auto item_of = [&](uint32_t k, uint32_t &xs, uint32_t &g, uint32_t &zs, uint32_t &ze, uint32_t &bz0,
+                       uint32_t &bz1) {
+        xs = k % a.nXS;
+        const uint32_t rest = k / a.nXS, zc = rest % a.nZC;
+        g = rest / a.nZC;
+        bz0 = zc * a.zchunk;
+        bz1 = min(a.GZ, bz0 + a.zchunk);
+        zs = bz0 * B;
+        ze = min(bz1 * B, a.Z - 1);
+    };
+    // producer cursor (thread 0 only): next slice to load
+    uint32_t pk = blockIdx.x, pz = 0, pze = 0, pxs = 0, pg = 0;
+    uint32_t issued = 0;  // slices issued so far
+    if (tid == 0 && pk < a.nitems) {
+        uint32_t b0, b1;
+        item_of(pk, pxs, pg, pz, pze, b0, b1);
+    }
+    auto issue_next = [&]() {  // thread 0: one slice into stage issued % S
+        if (pk >= a.nitems) return;
+        uint64_t *bar = &bars[issued % S];
+        unsigned char *dst = smem + (issued % S) * STAGE;
+        fence_proxy_async();
+        mbar_arrive_expect_tx(bar, TX);
+        const int x0 = (int)(pxs * SEG), y0 = (int)(pg * 4 * B);
+        tma_load_3d(dst, &map_main, bar, x0, y0, (int)pz);
+        tma_load_3d(dst + HOFF, &map_halo, bar, x0 + SEG, y0, (int)pz);
+        ++issued;
+        if (++pz > pze) {
+            pk += gridDim.x;
+            if (pk < a.nitems) {
+                uint32_t b0, b1;
+                item_of(pk, pxs, pg, pz, pze, b0, b1);
+            }
+        }
+    };
+    if (tid == 0)
+        for (int i = 0; i < S; ++i) issue_next();
+
+    uint32_t seq = 0;  // slices consumed
+    bool ok = true;
+    for (uint32_t k = blockIdx.x; k < a.nitems && ok; k += gridDim.x) {
+        uint32_t xs, g, zs, ze, bz0, bz1;
+        item_of(k, xs, g, zs, ze, bz0, bz1);
+        const uint32_t x0 = xs * SEG + lane * V;
+        const bool on = x0 < a.X;  // X is a multiple of V
+        const bool halo_on = lane == 31 && xs * SEG + SEG < a.X;
+        const uint32_t by = g * 4 + w;
+        const bool row_on = by < a.GY;
+        const uint32_t ny = row_on ? min((uint32_t)B + 1u, a.Y - by * B) : 0u;
+        uint32_t amn[NB], amx[NB];
+#pragma unroll
+        for (int j = 0; j < NB; ++j) { amn[j] = ~0u; amx[j] = 0u; }
+        uint32_t bz = bz0;
+        for (uint32_t z = zs; z <= ze; ++z, ++seq) {
+            if (!mbar_wait_bounded(&bars[seq % S], (seq / S) & 1u)) {
+                if (lane == 0) {
+                    report(st, MTX_ERR_TIMEOUT, kSiteMinMaxTma, blockIdx.x, seq);
+                    atomicExch(&s_fail, 1u);
+                }
+            }
+            const unsigned char *stg = smem + (seq % S) * STAGE;
+            // two independent folds (even and odd rows) halve the dependent chain
+            uint4 mn = L16::lo_id(), mx = L16::hi_id(), mn1 = L16::lo_id(), mx1 = L16::hi_id();
+            uint32_t hmn = ~0u, hmx = 0u;
+            if (on) {
+#pragma unroll
+                for (int r = 0; r <= B; ++r) {
+                    if ((uint32_t)r < ny) {
+                        const uint4 v = *reinterpret_cast<const uint4 *>(stg + (w * B + r) * 512u + lane * 16u);
+                        if (r & 1) L16::fold(mn1, mx1, v);
+                        else L16::fold(mn, mx, v);
+                    }
+                }
+                L16::merge(mn, mx, mn1, mx1);
+            }
+            if (halo_on) {
+#pragma unroll
+                for (int r = 0; r <= B; ++r) {
+                    if ((uint32_t)r < ny) {
+                        const uint32_t hk = Vox<T>::key(*reinterpret_cast<const T *>(stg + HOFF + (w * B + r) * 16u));
+                        hmn = min(hmn, hk);
+                        hmx = max(hmx, hk);
+                    }
+                }
+            }
+            // first column of the next lane is this lane's halo column
+            uint32_t nmn = __shfl_down_sync(0xffffffffu, L16::elem(mn, 0, false), 1);
+            uint32_t nmx = __shfl_down_sync(0xffffffffu, L16::elem(mx, 0, true), 1);
+            if (lane == 31) { nmn = hmn; nmx = hmx; }
+            uint32_t smn[NB], smx[NB];
+#pragma unroll
+            for (int j = 0; j < NB; ++j) {
+                uint32_t lo = ~0u, hi = 0u;
+                if constexpr (sizeof(T) == 2 && CNT == 8) {  // all 8 lanes of the word: a SIMD tree
+                    const uint32_t a2 = __vminu2(__vminu2(mn.x, mn.y), __vminu2(mn.z, mn.w));
+                    const uint32_t b2 = __vmaxu2(__vmaxu2(mx.x, mx.y), __vmaxu2(mx.z, mx.w));
+                    lo = min(a2 & 0xFFFFu, a2 >> 16);
+                    hi = max(b2 & 0xFFFFu, b2 >> 16);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < CNT; ++i) {
+                        lo = min(lo, L16::elem(mn, j * CNT + i, false));
+                        hi = max(hi, L16::elem(mx, j * CNT + i, true));
+                    }
+                }
+                const bool take_halo = V >= B ? true : ((lane % LPB) == LPB - 1);
+                if (take_halo) {
+                    if (V >= B && j + 1 < NB) {
+                        lo = min(lo, L16::elem(mn, (j + 1) * B, false));
+                        hi = max(hi, L16::elem(mx, (j + 1) * B, true));
+                    } else {
+                        lo = min(lo, nmn);
+                        hi = max(hi, nmx);
+                    }
+                }
+                smn[j] = lo;
+                smx[j] = hi;
+            }
+#pragma unroll
+            for (int j = 0; j < NB; ++j) { amn[j] = min(amn[j], smn[j]); amx[j] = max(amx[j], smx[j]); }
+            if (z == bz * B + B) {
+                // halo slice of bz, first slice of bz + 1: write block bz
+#pragma unroll
+                for (int j = 0; j < NB; ++j) {
+                    uint32_t lo = amn[j], hi = amx[j];
+#pragma unroll
+                    for (int o = 1; o < LPB; o <<= 1) {
+                        lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+                        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+                    }
+                    if (row_on && on && (lane % LPB) == 0)
+                        leaf[((uint64_t)bz * a.GY + by) * a.GX + x0 / B + j] = make_uint2(lo, hi);
+                    amn[j] = smn[j];
+                    amx[j] = smx[j];
+                }
+                ++bz;
+            }
+            __syncthreads();  // every warp is done with this stage
+            if (s_fail) {
+                ok = false;
+                ++seq;
+                break;
+            }
+            if (tid == 0) issue_next();
+        }
+        if (ok && bz < bz1) {
+#pragma unroll
+            for (int j = 0; j < NB; ++j) {
+                uint32_t lo = amn[j], hi = amx[j];
+#pragma unroll
+                for (int o = 1; o < LPB; o <<= 1) {
+                    lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+                    hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+                }
+                if (row_on && on && (lane % LPB) == 0)
+                    leaf[((uint64_t)bz * a.GY + by) * a.GX + x0 / B + j] = make_uint2(lo, hi);
+            }
+        }
+    }
+    // no copy may still be in flight into this CTA's shared memory when it exits
+    if (tid == 0)
+        for (; seq < issued; ++seq) mbar_wait_bounded(&bars[seq % S], (seq / S) & 1u);
+}
+
 // Fallback for any block edge and any row alignment: one thread per block.
 template <typename T>
 __global__ void __launch_bounds__(128) minmax_leaf_generic_kernel(const T *__restrict__ vol, uint32_t X,
@@ -105,6 +328,42 @@ static cudaError_t launch_generic(const Problem &p, uint2 *leaf, cudaStream_t s)
     return cudaGetLastError();
 }
 
+template <typename T, int B>
+static mtx_status launch_tma(mtx_context *c, const Problem &p, uint2 *leaf, cudaStream_t s, uint32_t zover) {
+    constexpr uint32_t SEG = 32 * (16 / sizeof(T));
+    CUtensorMap mmain, mhalo;
+    mtx_status r = make_volume_tensor_map_box(c, p, SEG, kTmaRows(B), 1, &mmain);
+    if (r == MTX_OK) r = make_volume_tensor_map_box(c, p, 16 / sizeof(T), kTmaRows(B), 1, &mhalo);
+    if (r != MTX_OK) return r;
+    TmaLeafArgs a;
+    a.X = p.X; a.Y = p.Y; a.Z = p.Z;
+    a.GX = p.GX; a.GY = p.GY; a.GZ = p.GZ;
+    a.nXS = ceil_div(p.X, SEG);
+    a.nYG = ceil_div(p.GY, 4);
+    // slab runs of 32 voxel slices (a 1/33 halo repeat, served by L2), fewer
+    // when the volume is too small to give every SM a few items
+    uint32_t zc = zover ? zover : std::max<uint32_t>(1, 32 / B);
+    if (!zover)
+        while (zc > 1 && (uint64_t)a.nXS * a.nYG * ceil_div(p.GZ, zc) < 4ull * kTmaCtasPerSm * c->sm_count)
+        zc = (zc + 1) / 2;
+    a.zchunk = zc;
+    a.nZC = ceil_div(p.GZ, zc);
+    a.nitems = a.nXS * a.nYG * a.nZC;
+    const uint32_t smem = kTmaStages(B) * kTmaStage(B);
+    auto k = minmax_leaf_tma_kernel<T, B>;
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return cuda_fail(c, e, "minmax tma attribute");
+    int occ = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, 128, smem);
+    if (e != cudaSuccess) return cuda_fail(c, e, "minmax tma occupancy");
+    occ = std::max(1, std::min(occ, kTmaCtasPerSm));
+    const uint32_t grid = std::min<uint32_t>(a.nitems, (uint32_t)c->sm_count * (uint32_t)occ);
+    k<<<grid, 128, smem, s>>>(mmain, mhalo, a, leaf, &c->ctrl->status);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(c, e, "minmax tma launch");
+    return MTX_OK;
+}
+
 template <typename T, int ZU>
 static cudaError_t dispatch_b(const Problem &p, uint2 *leaf, cudaStream_t s, int sm, uint32_t zover) {
     switch (p.B) {
@@ -131,6 +390,25 @@ mtx_status launch_minmax_leaf(mtx_context *c, const Problem &p, uint2 *leaf, cud
     cudaError_t e;
     if (!zover) zover = c->tuning.minmaxZChunk;
     const uint32_t sl = c->tuning.minmaxSlices;
+    // TMA ring (the default for 2- and 4-byte voxels whose rows are 16-byte
+    // aligned); the load-based body when tuning asks for 1, 2 or 4 slices
+    const uint32_t esz = dtype_size(p.dtype);
+    const bool tma = sl == 0 && esz >= 2 && (uintptr_t)p.vol % 16 == 0 && ((uint64_t)p.X * esz) % 16 == 0 &&
+                     (p.B == 4 || p.B == 8 || p.B == 16);
+    if (tma) {
+        if (p.dtype == MTX_DTYPE_U16) {
+            switch (p.B) {
+            case 4: return launch_tma<uint16_t, 4>(c, p, leaf, s, zover);
+            case 8: return launch_tma<uint16_t, 8>(c, p, leaf, s, zover);
+            default: return launch_tma<uint16_t, 16>(c, p, leaf, s, zover);
+            }
+        }
+        switch (p.B) {
+        case 4: return launch_tma<float, 4>(c, p, leaf, s, zover);
+        case 8: return launch_tma<float, 8>(c, p, leaf, s, zover);
+        default: return launch_tma<float, 16>(c, p, leaf, s, zover);
+        }
+    }
     switch (p.dtype) {
     case MTX_DTYPE_U8: e = dispatch_leaf<uint8_t>(p, leaf, s, c->sm_count, zover, sl); break;
     case MTX_DTYPE_U16: e = dispatch_leaf<uint16_t>(p, leaf, s, c->sm_count, zover, sl); break;

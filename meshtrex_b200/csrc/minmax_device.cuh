@@ -26,6 +26,10 @@ template <> struct Lane16<uint8_t> {
         mn.x = __vminu4(mn.x, v.x); mn.y = __vminu4(mn.y, v.y); mn.z = __vminu4(mn.z, v.z); mn.w = __vminu4(mn.w, v.w);
         mx.x = __vmaxu4(mx.x, v.x); mx.y = __vmaxu4(mx.y, v.y); mx.z = __vmaxu4(mx.z, v.z); mx.w = __vmaxu4(mx.w, v.w);
     }
+    __device__ __forceinline__ static void merge(uint4 &mn, uint4 &mx, const uint4 &mn2, const uint4 &mx2) {
+        mn.x = __vminu4(mn.x, mn2.x); mn.y = __vminu4(mn.y, mn2.y); mn.z = __vminu4(mn.z, mn2.z); mn.w = __vminu4(mn.w, mn2.w);
+        mx.x = __vmaxu4(mx.x, mx2.x); mx.y = __vmaxu4(mx.y, mx2.y); mx.z = __vmaxu4(mx.z, mx2.z); mx.w = __vmaxu4(mx.w, mx2.w);
+    }
     __device__ __forceinline__ static uint32_t elem(const uint4 &w, int i, bool is_max) {
         uint32_t word = (i >> 2) == 0 ? w.x : (i >> 2) == 1 ? w.y : (i >> 2) == 2 ? w.z : w.w;
         return (word >> (8 * (i & 3))) & 0xFFu;
@@ -39,6 +43,10 @@ template <> struct Lane16<uint16_t> {
     __device__ __forceinline__ static void fold(uint4 &mn, uint4 &mx, uint4 v) {
         mn.x = __vminu2(mn.x, v.x); mn.y = __vminu2(mn.y, v.y); mn.z = __vminu2(mn.z, v.z); mn.w = __vminu2(mn.w, v.w);
         mx.x = __vmaxu2(mx.x, v.x); mx.y = __vmaxu2(mx.y, v.y); mx.z = __vmaxu2(mx.z, v.z); mx.w = __vmaxu2(mx.w, v.w);
+    }
+    __device__ __forceinline__ static void merge(uint4 &mn, uint4 &mx, const uint4 &mn2, const uint4 &mx2) {
+        mn.x = __vminu2(mn.x, mn2.x); mn.y = __vminu2(mn.y, mn2.y); mn.z = __vminu2(mn.z, mn2.z); mn.w = __vminu2(mn.w, mn2.w);
+        mx.x = __vmaxu2(mx.x, mx2.x); mx.y = __vmaxu2(mx.y, mx2.y); mx.z = __vmaxu2(mx.z, mx2.z); mx.w = __vmaxu2(mx.w, mx2.w);
     }
     __device__ __forceinline__ static uint32_t elem(const uint4 &w, int i, bool is_max) {
         uint32_t word = (i >> 1) == 0 ? w.x : (i >> 1) == 1 ? w.y : (i >> 1) == 2 ? w.z : w.w;
@@ -56,6 +64,10 @@ template <> struct Lane16<float> {
         uint32_t k2 = Vox<float>::key(__uint_as_float(v.z)), k3 = Vox<float>::key(__uint_as_float(v.w));
         mn.x = min(mn.x, k0); mn.y = min(mn.y, k1); mn.z = min(mn.z, k2); mn.w = min(mn.w, k3);
         mx.x = max(mx.x, k0); mx.y = max(mx.y, k1); mx.z = max(mx.z, k2); mx.w = max(mx.w, k3);
+    }
+    __device__ __forceinline__ static void merge(uint4 &mn, uint4 &mx, const uint4 &mn2, const uint4 &mx2) {
+        mn.x = min(mn.x, mn2.x); mn.y = min(mn.y, mn2.y); mn.z = min(mn.z, mn2.z); mn.w = min(mn.w, mn2.w);
+        mx.x = max(mx.x, mx2.x); mx.y = max(mx.y, mx2.y); mx.z = max(mx.z, mx2.z); mx.w = max(mx.w, mx2.w);
     }
     __device__ __forceinline__ static uint32_t elem(const uint4 &w, int i, bool is_max) {
         return i == 0 ? w.x : i == 1 ? w.y : i == 2 ? w.z : w.w;

@@ -29,6 +29,7 @@ enum : uint32_t {
     kSiteCountOverflow = 6,
     kSiteBatched = 7,
     kSiteAdjoint = 8,
+    kSiteMinMaxTma = 9,
 };
 
 __device__ __forceinline__ void report(DevStatus *st, uint32_t code, uint32_t where, uint32_t i0 = 0,

@@ -151,5 +151,7 @@ mtx_status launch_emit(mtx_context *c, const Problem &p, const ExtractArgs &a, c
 bool tma_ok(const Problem &p);
 // Build the 3D tensor map of the volume with a (bx, B+1, B+1) box.
 mtx_status make_volume_tensor_map(mtx_context *c, const Problem &p, uint32_t box_x, CUtensorMap *map);
+mtx_status make_volume_tensor_map_box(mtx_context *c, const Problem &p, uint32_t box_x, uint32_t box_y,
+                                      uint32_t box_z, CUtensorMap *map);
 
 }  // namespace mtx

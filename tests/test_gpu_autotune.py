@@ -23,7 +23,8 @@ def test_autotune_picks_caches_and_reuses(ctx, oracle, tmp_path):
     vol = _gyroid((80, 72, 96))
     cache = str(tmp_path / "tune.txt")
     r1 = api.autotune(ctx, vol, 0.0, cache_path=cache, flags=L.AUTOTUNE_QUICK)
-    assert r1["fromCache"] == 0 and r1["candidates"] == 3 * 3 * 2 + 2
+    # block edge x warps x staging, then the load-based min/max pass with 1, 2, 4 slices
+    assert r1["fromCache"] == 0 and r1["candidates"] == 3 * 3 * 2 + 3
     assert r1["blockEdge"] in (4, 8, 16) and r1["ms"] > 0
     assert r1["tuning"]["extractWarps"] in (2, 4, 8) and r1["tuning"]["staging"] in (1, 2)
     lines = open(cache).read().splitlines()
