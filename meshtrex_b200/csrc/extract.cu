@@ -92,9 +92,12 @@ __global__ void __launch_bounds__(kScanThreads)
 }
 
 // -------------------------------------------------------------- emit pass
-// CPL: context voxels per lane, ceil((3B^2 + 3B + 1) / 32): 8 covers B <= 8, 32 covers B <= 16
+// CPL: context voxels per lane, ceil((3B^2 + 3B + 1) / 32): 8 covers B <= 8, 32 covers B <= 16.
+// The xyz form of B <= 8 fits in 80 registers without spilling (72), so five
+// CTAs of four warps share an SM (107 registers allowed four); the other forms
+// would spill under that bound.
 template <typename T, int CPL, bool TMA, bool GENERIC>
-__global__ void __launch_bounds__(kMaxWarps * 32)
+__global__ void __launch_bounds__(kMaxWarps * 32, (!GENERIC && CPL == 8) ? 3 : 1)
     pmb_emit_kernel(Problem p, const __grid_constant__ CUtensorMap map, const uint32_t *__restrict__ ids,
                     const uint32_t *__restrict__ rank_map, const uint32_t *__restrict__ count_ptr,
                     const mtx_meshlet_descriptor *__restrict__ desc, const uint32_t *__restrict__ faces,
