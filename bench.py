@@ -216,7 +216,7 @@ def launches_per_extraction(grid):
     while m > 1:
         m >>= 1
         levels += 1
-    return 1 + (levels + 1) // 3 + 1 + 2 + 1  # leaf, octree launches, filter, count + scan, emit
+    return 1 + (1 if levels > 1 else 0) + 1 + 2 + 1  # leaf, octree, filter, count + scan, emit
 
 
 def read_traffic():

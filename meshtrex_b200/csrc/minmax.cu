@@ -7,6 +7,7 @@
 // by two warps that run side by side, so DRAM sees each voxel once and L2
 // serves the repeat.
 #include <algorithm>
+#include <cstring>
 
 #include "minmax_device.cuh"
 
@@ -256,32 +257,44 @@ __global__ void __launch_bounds__(128) minmax_leaf_generic_kernel(const T *__res
     if (b < nblocks) minmax_leaf_one<T>(vol, X, Y, Z, B, GX, GY, b, leaf);
 }
 
-// Three octree levels per launch: a CTA of 512 threads loads an 8x8x8 tile
-// of level l and writes the 4^3, 2^3 and 1 texels it covers in levels l+1..l+3
-// (each texel the min/max of its up-to-8 children; children past the level's
-// extent are skipped, minMaxOctreeReduce.comp.glsl:37-47).
-struct PyrLevels {
-    uint2 *base[4];      // level l .. l+3
-    uint32_t ext[4][3];  // their extents
-    int nout;            // levels written (1..3)
+// Every octree level in one launch (minMaxOctreeReduce.comp.glsl:23-59 runs
+// one dispatch per level): a CTA of 512 threads loads an 8^3 tile of the leaf
+// level and writes the 4^3, 2^3 and 1 texels it covers in levels 1..3; the
+// CTA that finishes last builds levels 4.. from level 3 and zeroes the
+// counter (zero since the context's creation) for the next launch.  Each
+// texel is the min/max of its up-to-8 children; children past their level's
+// extent are skipped (minMaxOctreeReduce.comp.glsl:37-47), which the
+// identity {~0, 0} of the texels outside the leaf level's extent gives for
+// free.  The tile stays at 8^3 (4 KB of shared memory) so that the CTAs fit
+// beside the extraction kernels of other streams.
+constexpr int kPyrMaxLevels = 32;
+struct PyrAll {
+    uint2 *base[kPyrMaxLevels];
+    uint32_t ext[kPyrMaxLevels][3];
+    int levels;
 };
 
-__global__ void __launch_bounds__(512) pyramid3_kernel(PyrLevels L, uint32_t tiles_x, uint32_t tiles_y) {
+__global__ void __launch_bounds__(512) pyramid_all_kernel(const __grid_constant__ PyrAll L, uint32_t tiles_x,
+                                                          uint32_t tiles_y, uint32_t ntiles, uint32_t *done) {
     __shared__ uint2 s[512];
+    __shared__ uint32_t s_last;
+    const uint32_t t = threadIdx.x;
     const uint32_t tx = blockIdx.x % tiles_x, ty = (blockIdx.x / tiles_x) % tiles_y, tz = blockIdx.x / (tiles_x * tiles_y);
-    const uint32_t lx = threadIdx.x & 7, ly = (threadIdx.x >> 3) & 7, lz = threadIdx.x >> 6;
-    const uint32_t x = tx * 8 + lx, y = ty * 8 + ly, z = tz * 8 + lz;
-    uint2 v = make_uint2(~0u, 0u);
-    if (x < L.ext[0][0] && y < L.ext[0][1] && z < L.ext[0][2])
-        v = L.base[0][((uint64_t)z * L.ext[0][1] + y) * L.ext[0][0] + x];
-    s[threadIdx.x] = v;
+    {
+        const uint32_t x = tx * 8 + (t & 7), y = ty * 8 + ((t >> 3) & 7), z = tz * 8 + (t >> 6);
+        uint2 v = make_uint2(~0u, 0u);
+        if (x < L.ext[0][0] && y < L.ext[0][1] && z < L.ext[0][2])
+            v = L.base[0][((uint64_t)z * L.ext[0][1] + y) * L.ext[0][0] + x];
+        s[t] = v;
+    }
     __syncthreads();
+    const int top = min(3, L.levels - 1);
     uint32_t n = 8;  // current tile edge in shared memory
-    for (int k = 1; k <= L.nout; ++k) {
+    for (int k = 1; k <= top; ++k) {
         const uint32_t m = n >> 1;
         uint2 r = make_uint2(~0u, 0u);
-        const bool act = threadIdx.x < m * m * m;
-        const uint32_t cx = threadIdx.x % m, cy = (threadIdx.x / m) % m, cz = threadIdx.x / (m * m);
+        const bool act = t < m * m * m;
+        const uint32_t cx = t % m, cy = (t / m) % m, cz = t / (m * m);
         if (act) {
 #pragma unroll
             for (int c = 0; c < 8; ++c) {
@@ -292,7 +305,7 @@ __global__ void __launch_bounds__(512) pyramid3_kernel(PyrLevels L, uint32_t til
         }
         __syncthreads();
         if (act) {
-            s[threadIdx.x] = r;  // compact m^3 layout for the next level
+            s[t] = r;  // compact m^3 layout for the next level
             const uint32_t ox = tx * m + cx, oy = ty * m + cy, oz = tz * m + cz;
             if (ox < L.ext[k][0] && oy < L.ext[k][1] && oz < L.ext[k][2])
                 L.base[k][((uint64_t)oz * L.ext[k][1] + oy) * L.ext[k][0] + ox] = r;
@@ -300,6 +313,36 @@ __global__ void __launch_bounds__(512) pyramid3_kernel(PyrLevels L, uint32_t til
         __syncthreads();
         n = m;
     }
+    if (L.levels <= 4) return;
+    // level 3 of every tile is written: the last CTA to get here builds the rest
+    __threadfence();
+    __syncthreads();
+    if (t == 0) s_last = atomicAdd(done, 1u) == ntiles - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    for (int k = 4; k < L.levels; ++k) {
+        const uint32_t ex = L.ext[k][0], ey = L.ext[k][1], ez = L.ext[k][2];
+        const uint32_t px = L.ext[k - 1][0], py = L.ext[k - 1][1], pz = L.ext[k - 1][2];
+        const uint64_t cnt = (uint64_t)ex * ey * ez;
+        for (uint64_t i = t; i < cnt; i += 512) {
+            const uint32_t x = (uint32_t)(i % ex), y = (uint32_t)((i / ex) % ey), z = (uint32_t)(i / ((uint64_t)ex * ey));
+            uint2 r = make_uint2(~0u, 0u);
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                const uint32_t ux = 2 * x + (c & 1), uy = 2 * y + ((c >> 1) & 1), uz = 2 * z + (c >> 2);
+                if (ux < px && uy < py && uz < pz) {
+                    const uint2 w = __ldcg(&L.base[k - 1][((uint64_t)uz * py + uy) * px + ux]);
+                    r.x = min(r.x, w.x);
+                    r.y = max(r.y, w.y);
+                }
+            }
+            L.base[k][i] = r;
+        }
+        __threadfence();
+        __syncthreads();
+    }
+    if (t == 0) *done = 0;
 }
 
 // ------------------------------------------------------------------ host
@@ -420,19 +463,19 @@ mtx_status launch_minmax_leaf(mtx_context *c, const Problem &p, uint2 *leaf, cud
 
 mtx_status launch_pyramid(mtx_context *c, uint2 *all, int levels, const uint32_t ext[][3],
                           const uint64_t *offset, cudaStream_t s) {
-    for (int l = 0; l + 1 < levels; l += 3) {
-        PyrLevels P;
-        P.nout = std::min(3, levels - 1 - l);
-        for (int k = 0; k <= 3; ++k) {
-            const int lv = std::min(l + k, levels - 1);
-            P.base[k] = all + offset[lv];
-            for (int a = 0; a < 3; ++a) P.ext[k][a] = ext[lv][a];
-        }
-        const uint32_t tx = ceil_div(ext[l][0], 8), ty = ceil_div(ext[l][1], 8), tz = ceil_div(ext[l][2], 8);
-        pyramid3_kernel<<<tx * ty * tz, 512, 0, s>>>(P, tx, ty);
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess) return cuda_fail(c, e, "pyramid launch");
+    if (levels < 2) return MTX_OK;
+    if (levels > kPyrMaxLevels) return fail(c, MTX_ERR_UNSUPPORTED, "too many mip levels");
+    PyrAll P;
+    memset(&P, 0, sizeof(P));
+    P.levels = levels;
+    for (int k = 0; k < levels; ++k) {
+        P.base[k] = all + offset[k];
+        for (int a = 0; a < 3; ++a) P.ext[k][a] = ext[k][a];
     }
+    const uint32_t tx = ceil_div(ext[0][0], 8), ty = ceil_div(ext[0][1], 8), tz = ceil_div(ext[0][2], 8);
+    pyramid_all_kernel<<<tx * ty * tz, 512, 0, s>>>(P, tx, ty, tx * ty * tz, &c->ctrl->pyr_done);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(c, e, "pyramid launch");
     return MTX_OK;
 }
 

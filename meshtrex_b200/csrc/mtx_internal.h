@@ -21,6 +21,8 @@ struct Ctrl {
     uint32_t pad0;
     uint32_t totals[4];      // vertexCount, indexCount, meshletCount, activeBlockCount
     uint32_t batch_ticket[4];
+    uint32_t pyr_done;       // octree tiles finished (the last one builds the top levels)
+    uint32_t pad1[3];
 };
 
 // A grow-only device allocation owned by the context.
