@@ -452,7 +452,7 @@ __device__ __forceinline__ void batch_bases(const BatchArgs &a, uint32_t n, uint
 __device__ __forceinline__ void batch_count_block(const BatchArgs &a, const Problem &p, const WPlan &pl,
                                                   unsigned char *ws, const uint8_t *ntab, uint32_t id, uint32_t r) {
     const Geo g = block_geo(id, p, false, 4);
-    tile_load_float(p, pl, reinterpret_cast<float *>(ws + pl.off_tile[0]), g);
+    tile_load_rows(p, pl, ws, g);
     count_block_balanced(p, pl, ws, g, ntab, a.desc + r, a.faces + (uint64_t)r * a.face_stride);
 }
 
@@ -466,7 +466,7 @@ __device__ __forceinline__ void batch_emit_block(const BatchArgs &a, const Probl
     const mtx_meshlet_descriptor d{q.x, q.y, q.z, q.w};
     const uint32_t nb_rk = neighbour_rank<false>(p, g, id, a.rank_pool + rank_off);
     const uint32_t nb_vb = nb_rk != kNoVertex ? __ldcg(&a.desc[nb_rk].vertexOffset) : kNoVertex;
-    tile_load_float(p, pl, reinterpret_cast<float *>(ws + pl.off_tile[0]), g);
+    tile_load_rows(p, pl, ws, g);
     void *verts = a.vertices ? (void *)((char *)a.vertices + jr.vertexOffset * a.vsz) : nullptr;
     if (!emit_vertices_balanced<GENERIC>(p, pl, ws, g, d, ntab, jr.indexCount / 3u, verts, jr.vertexCount, a.vfmt,
                                          a.frame, a.normals, &a.ctrl->status, r))

@@ -63,6 +63,58 @@ __host__ __device__ inline WPlan make_wplan_balanced(uint32_t B) {
     return p;
 }
 
+// Plain loads of a block's (B+1)^3 tile as float (tile_load_float) that also
+// build its inside masks (build_rows<float>): the inside bits of 32
+// consecutive tile voxels -- in the volume and at or below the isovalue --
+// are one warp ballot, a word of the tile's bitstream (kept in the list
+// region, which is free until the block's cells are listed), and row (y, z)
+// is the B+1 bits from bit (z*(B+1) + y)*(B+1) on.  The layout's tile pitch
+// is B+1, so voxel i of the tile is tile[i].
+template <typename S>
+__device__ __forceinline__ void tile_load_rows_from(const Problem &p, const WPlan &pl, unsigned char *ws,
+                                                    const Geo &g) {
+    constexpr uint32_t kLdgBatch = 8;
+    const S *vol = reinterpret_cast<const S *>(p.vol);
+    float *tile = reinterpret_cast<float *>(ws + pl.off_tile[0]);
+    uint32_t *words = reinterpret_cast<uint32_t *>(ws + pl.off_list);
+    uint32_t *rows = reinterpret_cast<uint32_t *>(ws + pl.off_rows);
+    const uint32_t lane = threadIdx.x & 31, B1 = pl.B1, n = B1 * B1 * B1, nw = (n + 31) / 32;
+    for (uint32_t i0 = 0; i0 < n; i0 += 32 * kLdgBatch) {
+        float v[kLdgBatch];
+        bool in[kLdgBatch];
+#pragma unroll
+        for (uint32_t k = 0; k < kLdgBatch; ++k) {
+            const uint32_t i = i0 + k * 32 + lane;
+            const uint32_t iq = fdiv(i, pl.rB1);
+            const uint32_t x = i - iq * B1, z = fdiv(iq, pl.rB1), y = iq - z * B1;
+            const uint32_t gx = g.ox + x, gy = g.oy + y, gz = g.oz + z;
+            in[k] = i < n && gx < p.X && gy < p.Y && gz < p.Z;
+            v[k] = in[k] ? Vox<S>::val(__ldg(vol + ((uint64_t)gz * p.Y + gy) * p.X + gx)) : 0.0f;
+        }
+#pragma unroll
+        for (uint32_t k = 0; k < kLdgBatch; ++k) {
+            const uint32_t i = i0 + k * 32 + lane, w = (i0 >> 5) + k;
+            if (i < n) tile[i] = v[k];
+            const uint32_t bal = __ballot_sync(0xffffffffu, in[k] && v[k] <= p.iso);
+            if (lane == 0 && w < nw) words[w] = bal;
+        }
+    }
+    __syncwarp();
+    const uint32_t mask = (1u << B1) - 1u;
+    for (uint32_t q = lane; q < B1 * B1; q += 32) {
+        const uint32_t bit = q * B1, w = bit >> 5;
+        const uint64_t two = (uint64_t)words[w] | (w + 1 < nw ? (uint64_t)words[w + 1] << 32 : 0ull);
+        rows[q] = (uint32_t)(two >> (bit & 31)) & mask;
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ void tile_load_rows(const Problem &p, const WPlan &pl, unsigned char *ws, const Geo &g) {
+    if (p.dtype == MTX_DTYPE_U8) tile_load_rows_from<uint8_t>(p, pl, ws, g);
+    else if (p.dtype == MTX_DTYPE_U16) tile_load_rows_from<uint16_t>(p, pl, ws, g);
+    else tile_load_rows_from<float>(p, pl, ws, g);
+}
+
 // Cell (x, y, z) of linear index c (x fastest) of a B^3 block.
 __device__ __forceinline__ void cell_xyz(const WPlan &pl, uint32_t c, uint32_t &x, uint32_t &y, uint32_t &z) {
     const uint32_t q = fdiv(c, pl.rB);
@@ -151,14 +203,14 @@ __device__ __forceinline__ void block_counts_balanced(const Problem &p, const WP
     }
 }
 
-// Count body (count_block) with the balanced triangle count.
+// Count body (count_block) with the balanced triangle count, for a block
+// whose tile and inside masks tile_load_rows staged.
 __device__ __forceinline__ void count_block_balanced(const Problem &p, const WPlan &pl, unsigned char *ws,
                                                      const Geo &g, const uint8_t *ntab, mtx_meshlet_descriptor *dr,
                                                      uint32_t *fr) {
     const uint32_t lane = threadIdx.x & 31, B = pl.B, BB = pl.BB;
     const uint32_t *cross = reinterpret_cast<const uint32_t *>(ws + pl.off_cross);
     const uint32_t *vp = reinterpret_cast<const uint32_t *>(ws + pl.off_vp);
-    build_rows<float>(p, pl, ws, 0, g);
     uint32_t bnv, bnt;
     block_counts_balanced(p, pl, ws, g, ntab, true, bnv, bnt);
     if (lane == 0) *reinterpret_cast<uint2 *>(&dr->vertexCount) = make_uint2(bnv, bnt);
@@ -323,7 +375,6 @@ __device__ __forceinline__ bool emit_vertices_balanced(const Problem &p, const W
         return false;
     }
     if (!(d.primitiveCount || (vertices && d.vertexCount))) return false;
-    build_rows<float>(p, pl, ws, 0, g);
     uint32_t bnv, bnt;
     block_counts_balanced(p, pl, ws, g, ntab, false, bnv, bnt);
     if (lane == 0 && bnv != d.vertexCount) report(st, MTX_ERR_INTERNAL, kSiteEmitNeighbour, r, 2);
