@@ -629,8 +629,6 @@ WPlan plan_in_layout(uint32_t B, const WPlan &L) {
     p.off_vp = L.off_vp;
     p.off_list = L.off_list;
     p.off_vmsk = L.off_vmsk;
-    p.off_stage = L.off_stage;
-    p.off_tstage = L.off_tstage;
     p.off_jobs = L.off_jobs;
     p.bytes = L.bytes;
     return p;

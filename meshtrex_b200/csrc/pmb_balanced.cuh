@@ -12,11 +12,10 @@
 // Layout (make_wplan_balanced): a single float tile, which the vertex table
 // takes over once the block's vertices are written; the context layer of the
 // table is gathered from the neighbours' face records at that point.  The
-// staging of 32 vertices lives in the owned-edge masks (written after the
-// vertices), that of 32 triangles in the crossing rows (dead once the table
-// is filled), and the row prefixes in the job ring (dead until the first job
-// is queued), so that four CTAs of eight warps fit an SM at B = 8.  Same
-// output as the row bodies, bit for bit.
+// row prefixes live in the job ring (dead until the first job is queued),
+// and outputs go straight from the lanes to global memory, so that four CTAs
+// of eight warps fit an SM at B = 8.  Same output as the row bodies, bit for
+// bit.
 #pragma once
 
 #include "pmb_device.cuh"
@@ -36,7 +35,7 @@ __host__ __device__ inline WPlan make_wplan_balanced(uint32_t B) {
     p.rBB = (uint32_t)((0x100000000ull + B * B - 1) / (B * B));
     p.R = 32 / B;
     p.PX = B + 1;
-    const uint32_t T3 = p.B1 * p.B1 * p.B1, stage = 4 * kStageWords;
+    const uint32_t T3 = p.B1 * p.B1 * p.B1;
     p.tile_bytes = 4 * T3;
     p.nbuf = 1;
     uint32_t o = 0;
@@ -55,9 +54,6 @@ __host__ __device__ inline WPlan make_wplan_balanced(uint32_t B) {
     p.off_jobs = o;
     o = align_up(o + 4 * kRing, 16);
     p.off_vp = p.off_jobs;  // 4 * BB <= 4 * kRing for B <= 16
-    p.off_stage = T3 >= stage ? p.off_vmsk : o;
-    p.off_tstage = 12 * p.BB >= stage ? p.off_cross : o;
-    if (T3 < stage || 12 * p.BB < stage) o = align_up(o + stage, 16);
     p.off_nvid = p.off_nm = p.off_tp = 0;  // unused
     p.bytes = o;
     return p;
@@ -301,7 +297,6 @@ __device__ __forceinline__ void resolve_vertices(const Problem &p, const WPlan &
                                                  uint32_t vfmt, uint32_t frame, uint32_t normals) {
     const uint32_t lane = threadIdx.x & 31, B1 = pl.B1;
     const float *tile = reinterpret_cast<const float *>(ws + pl.off_tile[0]);
-    float *stage = reinterpret_cast<float *>(ws + pl.off_stage);
     const uint32_t *jobs = reinterpret_cast<const uint32_t *>(ws + pl.off_jobs);
     const bool xyz = !GENERIC || vfmt == MTX_VERTEX_XYZ;
     if (lane < n) {
@@ -311,10 +306,11 @@ __device__ __forceinline__ void resolve_vertices(const Problem &p, const WPlan &
         const uint32_t x = t3 - iq * B1, z = fdiv(iq, pl.rB1), y = iq - z * B1;
         float t;
         const float3 pos = vertex_pos<float>(p, pl, tile, g, x, y, z, a, GENERIC && frame == MTX_FRAME_NDC, &t);
-        if (xyz) {
-            stage[3 * lane + 0] = pos.x;
-            stage[3 * lane + 1] = pos.y;
-            stage[3 * lane + 2] = pos.z;
+        if (xyz) {  // each lane its own 12 bytes, as the triangles
+            float *o = reinterpret_cast<float *>(vertices) + 3ull * (vbase + done + lane);
+            o[0] = pos.x;
+            o[1] = pos.y;
+            o[2] = pos.z;
         } else {
             float3 nn = make_float3(0.0f, 0.0f, 0.0f);
             if (normals) nn = vertex_normal_any(p, g.ox + x, g.oy + y, g.oz + z, a, t);
@@ -322,11 +318,6 @@ __device__ __forceinline__ void resolve_vertices(const Problem &p, const WPlan &
             o[0] = make_float4(pos.x, pos.y, pos.z, 1.0f);
             o[1] = make_float4(nn.x, nn.y, nn.z, 0.0f);
         }
-    }
-    __syncwarp();
-    if (xyz) {
-        float *dst = reinterpret_cast<float *>(vertices) + 3ull * (vbase + done);
-        for (uint32_t w = lane; w < 3 * n; w += 32) dst[w] = stage[w];
     }
     __syncwarp();
 }
@@ -339,18 +330,17 @@ __device__ __forceinline__ void resolve_triangles(const WPlan &pl, unsigned char
     const uint32_t lane = threadIdx.x & 31, B1 = pl.B1;
     const uint32_t *vtab = reinterpret_cast<const uint32_t *>(ws + pl.off_vtab);
     const uint8_t *vmsk = ws + pl.off_vmsk;
-    uint32_t *stage = reinterpret_cast<uint32_t *>(ws + pl.off_tstage);
     const uint32_t *jobs = reinterpret_cast<const uint32_t *>(ws + pl.off_jobs);
+    // each lane stores its own 12 bytes: the warp's stores cover one 384-byte
+    // span, which L2 merges, and no staging round trip is spent
     if (lane < n) {
         const uint32_t job = jobs[(done + lane) & (kRing - 1)];
         const uint32_t cell = job & 0x1fffu, t = (job >> 13) & 7u;
         const uint64_t w = tab[job >> 16] >> (4 + 12 * t);
-        stage[3 * lane + 0] = table_vertex(cell, (uint32_t)(w & 0xFu), owner, B1, vtab, vmsk, bad);
-        stage[3 * lane + 1] = table_vertex(cell, (uint32_t)((w >> 4) & 0xFu), owner, B1, vtab, vmsk, bad);
-        stage[3 * lane + 2] = table_vertex(cell, (uint32_t)((w >> 8) & 0xFu), owner, B1, vtab, vmsk, bad);
+        dst[3 * lane + 0] = table_vertex(cell, (uint32_t)(w & 0xFu), owner, B1, vtab, vmsk, bad);
+        dst[3 * lane + 1] = table_vertex(cell, (uint32_t)((w >> 4) & 0xFu), owner, B1, vtab, vmsk, bad);
+        dst[3 * lane + 2] = table_vertex(cell, (uint32_t)((w >> 8) & 0xFu), owner, B1, vtab, vmsk, bad);
     }
-    __syncwarp();
-    for (uint32_t q = lane; q < 3 * n; q += 32) dst[q] = stage[q];
     __syncwarp();
 }
 

@@ -35,7 +35,6 @@ constexpr uint32_t kNoVertex = 0xffffffffu;
 // that every warp's region -- and the TMA tile at its start -- is 128-byte aligned
 constexpr uint32_t kTableBytes = 2432;
 static_assert(kTableBytes % 128 == 0 && kTableBytes >= 2048 + 256 + 16, "table region must keep warp regions aligned");
-constexpr uint32_t kStageWords = 32 * 3;           // one batch: 32 triangles x 3 indices or 32 xyz
 constexpr uint32_t kJobWin = 256;                   // jobs (vertices or triangles) resolved per window
 constexpr int kMaxWarps = 8;                        // warps per CTA of the extraction kernels
 
@@ -46,8 +45,8 @@ struct WPlan {
     uint32_t B, B1, BB, PX, nbuf, nb3;
     uint32_t rB, rB1, rBB;  // ceil(2^32 / d) reciprocals: n / d == __umulhi(n, r) for the sizes used here
     uint32_t R;             // block rows walked per round of 32 lanes (32 / B)
-    uint32_t off_tile[2], off_bar, off_rows, off_cross, off_vp, off_tp, off_nvid, off_nm, off_stage, off_jobs;
-    uint32_t off_vtab, off_vmsk, off_list, off_tstage;  // balanced bodies only (pmb_balanced.cuh)
+    uint32_t off_tile[2], off_bar, off_rows, off_cross, off_vp, off_tp, off_nvid, off_nm, off_jobs;
+    uint32_t off_vtab, off_vmsk, off_list;  // balanced bodies only (pmb_balanced.cuh)
     uint32_t bytes;       // per warp
     uint32_t tile_bytes;  // one tile (the TMA transaction size)
 };
@@ -98,8 +97,6 @@ __host__ __device__ inline WPlan make_wplan(uint32_t B, uint32_t esz, bool tma, 
         p.off_nm = o;
         o = align_up(o + p.nb3, 16);
     }
-    p.off_stage = o;
-    o = align_up(o + 4 * kStageWords, 16);
     p.off_jobs = o;  // a window of packed jobs (triangles or vertices) in output order
     o = align_up(o + 4 * kJobWin, 16);
     p.bytes = align_up(o, 128);
@@ -513,7 +510,6 @@ __device__ __forceinline__ void emit_vertices(const Problem &p, const WPlan &pl,
     const uint32_t *cross = reinterpret_cast<const uint32_t *>(ws + pl.off_cross);
     const uint32_t *vp = reinterpret_cast<const uint32_t *>(ws + pl.off_vp);
     const T *tile = reinterpret_cast<const T *>(ws + pl.off_tile[buf]);
-    float *stage = reinterpret_cast<float *>(ws + pl.off_stage);
     uint32_t *jobs = reinterpret_cast<uint32_t *>(ws + pl.off_jobs);
     const bool xyz = !GENERIC || vfmt == MTX_VERTEX_XYZ;
     for (uint32_t w0 = 0; w0 < nv; w0 += kJobWin) {
@@ -546,10 +542,11 @@ __device__ __forceinline__ void emit_vertices(const Problem &p, const WPlan &pl,
                 float t;
                 const float3 pos =
                     vertex_pos<T>(p, pl, tile, g, x, y, z, a, GENERIC && frame == MTX_FRAME_NDC, &t);
-                if (xyz) {
-                    stage[3 * lane + 0] = pos.x;
-                    stage[3 * lane + 1] = pos.y;
-                    stage[3 * lane + 2] = pos.z;
+                if (xyz) {  // each lane its own 12 bytes: L2 merges the warp's 384-byte span
+                    float *o = reinterpret_cast<float *>(vertices) + 3ull * (vbase + w0 + b + lane);
+                    o[0] = pos.x;
+                    o[1] = pos.y;
+                    o[2] = pos.z;
                 } else {
                     float3 nn = make_float3(0.0f, 0.0f, 0.0f);
                     if (normals) {
@@ -560,11 +557,6 @@ __device__ __forceinline__ void emit_vertices(const Problem &p, const WPlan &pl,
                     v[0] = make_float4(pos.x, pos.y, pos.z, 1.0f);
                     v[1] = make_float4(nn.x, nn.y, nn.z, 0.0f);
                 }
-            }
-            __syncwarp();
-            if (xyz) {
-                float *dst = reinterpret_cast<float *>(vertices) + 3ull * (vbase + w0 + b);
-                for (uint32_t w = lane; w < 3 * n; w += 32) dst[w] = stage[w];
             }
             __syncwarp();
         }
@@ -804,7 +796,6 @@ __device__ __forceinline__ void emit_block(const Problem &p, const WPlan &pl, un
     const uint32_t *tp = reinterpret_cast<const uint32_t *>(ws + pl.off_tp);
     const uint32_t *nvid = reinterpret_cast<const uint32_t *>(ws + pl.off_nvid);
     const uint8_t *nm = ws + pl.off_nm;
-    uint32_t *stage = reinterpret_cast<uint32_t *>(ws + pl.off_stage);
     uint32_t *jobs = reinterpret_cast<uint32_t *>(ws + pl.off_jobs);
     const uint32_t tbase = d.indexOffset / 3u;
     if ((uint64_t)tbase + d.primitiveCount > tcap || (vertices && (uint64_t)d.vertexOffset + d.vertexCount > vcap)) {
@@ -855,16 +846,14 @@ __device__ __forceinline__ void emit_block(const Problem &p, const WPlan &pl, un
                 const uint32_t q = fdiv(i, pl.rB), x = i - q * B;
                 const uint32_t z = fdiv(q, pl.rB), y = q - z * B;
                 const uint64_t w = tab[job >> 16] >> (4 + 12 * t);
-                stage[3 * lane + 0] = edge_vertex(x, y, z, (uint32_t)(w & 0xFu), owner, cross, vp, nvid, nm, B, BB,
-                                                  d.vertexOffset, bad);
-                stage[3 * lane + 1] = edge_vertex(x, y, z, (uint32_t)((w >> 4) & 0xFu), owner, cross, vp, nvid, nm,
-                                                  B, BB, d.vertexOffset, bad);
-                stage[3 * lane + 2] = edge_vertex(x, y, z, (uint32_t)((w >> 8) & 0xFu), owner, cross, vp, nvid, nm,
-                                                  B, BB, d.vertexOffset, bad);
+                uint32_t *o = indices + 3ull * (tbase + w0 + b + lane);  // each lane its own 12 bytes
+                o[0] = edge_vertex(x, y, z, (uint32_t)(w & 0xFu), owner, cross, vp, nvid, nm, B, BB, d.vertexOffset,
+                                   bad);
+                o[1] = edge_vertex(x, y, z, (uint32_t)((w >> 4) & 0xFu), owner, cross, vp, nvid, nm, B, BB,
+                                   d.vertexOffset, bad);
+                o[2] = edge_vertex(x, y, z, (uint32_t)((w >> 8) & 0xFu), owner, cross, vp, nvid, nm, B, BB,
+                                   d.vertexOffset, bad);
             }
-            __syncwarp();
-            uint32_t *dst = indices + 3ull * (tbase + w0 + b);
-            for (uint32_t q = lane; q < 3 * n; q += 32) dst[q] = stage[q];
             __syncwarp();
         }
     }
