@@ -5,9 +5,11 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <new>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "mtx_internal.h"
@@ -47,23 +49,122 @@ mtx_status cuda_fail(mtx_context *c, cudaError_t e, const char *what) {
 }
 
 // ----------------------------------------------------------------- memory
+// Freed device buffers are kept for reuse.  The drop-in stages allocate their
+// outputs per call, as meshtrex's managers do, and cudaMalloc / cudaFree of
+// the same sizes call after call cost host time: milliseconds for a 2 GiB
+// volume, many more on a busy host.  A freed buffer first waits for its
+// device to go idle -- the guarantee cudaFree gives, that no stream still
+// uses it -- and then goes to a per-device list by exact size, from which an
+// allocation of that size takes it back.  At most kCacheBytes and
+// kCacheBuffers are kept per device; a failed cudaMalloc hands the device's
+// cached buffers back to the driver and tries again, and so does the
+// destruction of a context (dev_cache_release).
+namespace {
+constexpr size_t kCacheBytes = 16ull << 30;
+constexpr uint32_t kCacheBuffers = 64;
+constexpr int kCacheDevices = 128;
+struct LiveAlloc {
+    int device;
+    size_t bytes;
+};
+std::mutex g_alloc_mu;
+std::unordered_map<void *, LiveAlloc> g_live;                // every buffer dev_alloc handed out
+std::map<std::pair<int, size_t>, std::vector<void *>> g_idle;  // (device, bytes) -> freed buffers
+size_t g_idle_bytes[kCacheDevices];
+uint32_t g_idle_count[kCacheDevices];
+
+void *take_idle(int device, size_t bytes) {
+    std::lock_guard<std::mutex> lk(g_alloc_mu);
+    auto it = g_idle.find({device, bytes});
+    if (it == g_idle.end() || it->second.empty()) return nullptr;
+    void *p = it->second.back();
+    it->second.pop_back();
+    g_idle_bytes[device] -= bytes;
+    --g_idle_count[device];
+    return p;
+}
+}  // namespace
+
+// Hands the freed buffers of `device` back to the driver (that device current).
+void dev_cache_release(int device) {
+    std::vector<void *> drop;
+    {
+        std::lock_guard<std::mutex> lk(g_alloc_mu);
+        for (auto it = g_idle.begin(); it != g_idle.end();) {
+            if (it->first.first == device) {
+                for (void *p : it->second) {
+                    drop.push_back(p);
+                    g_live.erase(p);
+                }
+                it = g_idle.erase(it);
+            } else {
+                ++it;
+            }
+        }
+        if (device >= 0 && device < kCacheDevices) {
+            g_idle_bytes[device] = 0;
+            g_idle_count[device] = 0;
+        }
+    }
+    for (void *p : drop) cudaFree(p);
+}
+
 mtx_status dev_alloc(mtx_context *c, void **p, size_t bytes) {
     *p = nullptr;
     if (c->fail_alloc_in) {
         if (--c->fail_alloc_in == 0) return fail(c, MTX_ERR_OOM, "injected allocation failure");
     }
     if (bytes == 0) bytes = 16;
+    const bool cached = c->device >= 0 && c->device < kCacheDevices;
+    if (cached && (*p = take_idle(c->device, bytes))) return MTX_OK;
     cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess && cached) {
+        cudaGetLastError();
+        dev_cache_release(c->device);
+        e = cudaMalloc(p, bytes);
+    }
     if (e != cudaSuccess) {
         *p = nullptr;
         cudaGetLastError();
         return fail(c, MTX_ERR_OOM, "cudaMalloc of " + std::to_string(bytes) + " bytes failed");
     }
+    if (cached) {
+        std::lock_guard<std::mutex> lk(g_alloc_mu);
+        g_live[*p] = LiveAlloc{c->device, bytes};
+    }
     return MTX_OK;
 }
 
 void dev_free(void *p) {
-    if (p) cudaFree(p);
+    if (!p) return;
+    LiveAlloc a{-1, 0};
+    {
+        std::lock_guard<std::mutex> lk(g_alloc_mu);
+        auto it = g_live.find(p);
+        if (it != g_live.end()) a = it->second;
+    }
+    if (a.device < 0) {
+        cudaFree(p);
+        return;
+    }
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (cur != a.device) cudaSetDevice(a.device);
+    cudaDeviceSynchronize();  // as cudaFree: no stream may still use the buffer
+    bool keep = false;
+    {
+        std::lock_guard<std::mutex> lk(g_alloc_mu);
+        if (g_idle_bytes[a.device] + a.bytes <= kCacheBytes && g_idle_count[a.device] < kCacheBuffers) {
+            g_idle[{a.device, a.bytes}].push_back(p);
+            g_idle_bytes[a.device] += a.bytes;
+            ++g_idle_count[a.device];
+            keep = true;
+        } else {
+            g_live.erase(p);
+        }
+    }
+    if (!keep) cudaFree(p);
+    if (cur >= 0 && cur != a.device) cudaSetDevice(cur);
 }
 
 mtx_status scratch_reserve(mtx_context *c, Scratch &s, size_t bytes) {
@@ -278,6 +379,7 @@ mtx_status mtx_context_destroy(mtx_context_t c) {
     for (Scratch *s : {&c->filter_status, &c->count_status, &c->faces, &c->leaf, &c->ids, &c->rank, &c->desc, &c->misc,
                        &c->adj_partial, &c->adj_iso})
         dev_free(s->ptr);
+    dev_cache_release(c->device);
     cudaFree(c->ctrl);
     cudaFreeHost(c->pinned);
     delete c;
