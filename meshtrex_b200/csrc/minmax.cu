@@ -144,19 +144,19 @@ __global__ void __launch_bounds__(128) minmax_leaf_tma_kernel(const __grid_const
                 }
             }
             const unsigned char *stg = smem + (seq % S) * STAGE;
-            // two independent folds (even and odd rows) halve the dependent chain
-            uint4 mn = L16::lo_id(), mx = L16::hi_id(), mn1 = L16::lo_id(), mx1 = L16::hi_id();
+            // row 0, then two rows per three-input min/max; rows past the volume
+            // read row 0 again, which leaves min and max unchanged
+            uint4 mn = L16::lo_id(), mx = L16::hi_id();
             uint32_t hmn = ~0u, hmx = 0u;
             if (on) {
+                const unsigned char *src = stg + w * B * 512u + lane * 16u;
+                auto row = [&](int r) {
+                    return *reinterpret_cast<const uint4 *>(src + ((uint32_t)r < ny ? (uint32_t)r : 0u) * 512u);
+                };
+                L16::init(mn, mx, row(0));
 #pragma unroll
-                for (int r = 0; r <= B; ++r) {
-                    if ((uint32_t)r < ny) {
-                        const uint4 v = *reinterpret_cast<const uint4 *>(stg + (w * B + r) * 512u + lane * 16u);
-                        if (r & 1) L16::fold(mn1, mx1, v);
-                        else L16::fold(mn, mx, v);
-                    }
-                }
-                L16::merge(mn, mx, mn1, mx1);
+                for (int r = 1; r + 1 <= B; r += 2) L16::fold2(mn, mx, row(r), row(r + 1));
+                if constexpr (B % 2 == 1) L16::fold2(mn, mx, row(B), row(B));
             }
             if (halo_on) {
 #pragma unroll

@@ -52,6 +52,14 @@ template <> struct Lane16<uint16_t> {
         uint32_t word = (i >> 1) == 0 ? w.x : (i >> 1) == 1 ? w.y : (i >> 1) == 2 ? w.z : w.w;
         return (word >> (16 * (i & 1))) & 0xFFFFu;
     }
+    __device__ __forceinline__ static void init(uint4 &mn, uint4 &mx, uint4 v) { mn = v; mx = v; }
+    // two rows per instruction: three-input packed min/max
+    __device__ __forceinline__ static void fold2(uint4 &mn, uint4 &mx, uint4 a, uint4 b) {
+        mn.x = __vimin3_u16x2(mn.x, a.x, b.x); mn.y = __vimin3_u16x2(mn.y, a.y, b.y);
+        mn.z = __vimin3_u16x2(mn.z, a.z, b.z); mn.w = __vimin3_u16x2(mn.w, a.w, b.w);
+        mx.x = __vimax3_u16x2(mx.x, a.x, b.x); mx.y = __vimax3_u16x2(mx.y, a.y, b.y);
+        mx.z = __vimax3_u16x2(mx.z, a.z, b.z); mx.w = __vimax3_u16x2(mx.w, a.w, b.w);
+    }
 };
 
 template <> struct Lane16<float> {
@@ -71,6 +79,18 @@ template <> struct Lane16<float> {
     }
     __device__ __forceinline__ static uint32_t elem(const uint4 &w, int i, bool is_max) {
         return i == 0 ? w.x : i == 1 ? w.y : i == 2 ? w.z : w.w;
+    }
+    __device__ __forceinline__ static uint4 keys(uint4 v) {
+        return make_uint4(Vox<float>::key(__uint_as_float(v.x)), Vox<float>::key(__uint_as_float(v.y)),
+                          Vox<float>::key(__uint_as_float(v.z)), Vox<float>::key(__uint_as_float(v.w)));
+    }
+    __device__ __forceinline__ static void init(uint4 &mn, uint4 &mx, uint4 v) { mn = mx = keys(v); }
+    __device__ __forceinline__ static void fold2(uint4 &mn, uint4 &mx, uint4 a, uint4 b) {
+        const uint4 ka = keys(a), kb = keys(b);
+        mn.x = __vimin3_u32(mn.x, ka.x, kb.x); mn.y = __vimin3_u32(mn.y, ka.y, kb.y);
+        mn.z = __vimin3_u32(mn.z, ka.z, kb.z); mn.w = __vimin3_u32(mn.w, ka.w, kb.w);
+        mx.x = __vimax3_u32(mx.x, ka.x, kb.x); mx.y = __vimax3_u32(mx.y, ka.y, kb.y);
+        mx.z = __vimax3_u32(mx.z, ka.z, kb.z); mx.w = __vimax3_u32(mx.w, ka.w, kb.w);
     }
 };
 

@@ -142,11 +142,39 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Waits for the phase with the given parity; false after the spin limit.
+// try_wait with a suspend-time hint: a thread whose phase is not complete is
+// suspended (issues nothing) until the phase completes or `ns` nanoseconds pass.
+__device__ __forceinline__ bool mbar_try_wait_for(uint64_t *bar, uint32_t parity, uint32_t ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(ns)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+constexpr uint32_t kMbarSuspendNs = 1u << 20;          // about 1 ms per try
+constexpr uint64_t kMbarWaitLimitNs = 2000000000ull;  // 2 s in all
+
+// Waits for the phase with the given parity; false after about 2 s (by the
+// global timer, or kSpinLimit tries should the timer not advance).  Waiting
+// warps sleep in try_wait instead of polling, so that the warps with work
+// get the issue slots.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = globaltimer_ns();
     for (uint32_t it = 0; it < kSpinLimit; ++it) {
-        if (mbar_try_wait(bar, parity)) return true;
-        backoff(it);
+        if (mbar_try_wait_for(bar, parity, kMbarSuspendNs)) return true;
+        if (globaltimer_ns() - t0 > kMbarWaitLimitNs) return false;
     }
     return false;
 }
