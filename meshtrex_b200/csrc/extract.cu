@@ -115,12 +115,14 @@ __global__ void __launch_bounds__(kMaxWarps * 32, (!GENERIC && CPL == 8) ? 3 : 1
     uint64_t *tab = reinterpret_cast<uint64_t *>(smem);
     uint8_t *ntab = smem + 2048;
     uint8_t *owner = smem + 2048 + 256;
+    uint32_t *cmap = reinterpret_cast<uint32_t *>(smem + kTableBytes);
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, W = blockDim.x >> 5;
-    unsigned char *ws = smem + kTableBytes + warp * pl.bytes;
+    unsigned char *ws = smem + cta_fixed_bytes(p.B, true) + warp * pl.bytes;
     for (uint32_t i = threadIdx.x; i < 256; i += blockDim.x) {
         tab[i] = c_mc_cases[i];
         ntab[i] = (uint8_t)(c_mc_cases[i] & 0xFu);
     }
+    for (uint32_t j = threadIdx.x; j < pl.nb3; j += blockDim.x) cmap[j] = ctx_map_entry(pl, j);
     if (threadIdx.x < 12) owner[threadIdx.x] = c_mc_owner[threadIdx.x];
     if (lane == 0 && TMA) {
         uint64_t *bar = reinterpret_cast<uint64_t *>(ws + pl.off_bar);
@@ -161,7 +163,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32, (!GENERIC && CPL == 8) ? 3 : 1
         }
         const uint32_t nb_vb = (nb_rk != kNoVertex) ? __ldg(&desc[nb_rk].vertexOffset) : kNoVertex;
         uint32_t rec[CPL];
-        gather_issue<CPL>(p, pl, g, nb_rk, faces, 3 * pl.BB, rec);
+        gather_issue_map<CPL>(p, pl, g, nb_rk, faces, 3 * pl.BB, cmap, rec);
         if (!tile_wait<T, TMA>(p, pl, ws, buf, g, parity, st)) {
             if (have_next && pl.nbuf == 2) tile_drain<TMA>(pl, ws, buf ^ 1u, parity);
             break;
@@ -231,7 +233,7 @@ template <typename T>
 static mtx_status run_emit(mtx_context *c, const Problem &p, const ExtractArgs &a, const CUtensorMap &map, bool tma,
                            uint32_t W, cudaStream_t s) {
     const WPlan pl = make_wplan(p.B, sizeof(T), tma, true, kSingleBuffer);
-    const uint32_t smem = kTableBytes + W * pl.bytes;
+    const uint32_t smem = cta_fixed_bytes(p.B, true) + W * pl.bytes;
     const bool generic = a.vertices && (a.vertex_format != MTX_VERTEX_XYZ || a.frame != MTX_FRAME_VOXEL);
     auto k = p.B <= 8 ? (tma ? emit_fn<T, 8, true>(generic) : emit_fn<T, 8, false>(generic))
                       : (tma ? emit_fn<T, 32, true>(generic) : emit_fn<T, 32, false>(generic));
@@ -264,7 +266,8 @@ static mtx_status launch_stage(mtx_context *c, const Problem &p, const ExtractAr
     W = std::min<uint32_t>(std::max<uint32_t>(W, 1), kMaxWarps);
     // no more warps than the shared memory holds (16^3 float tiles fit 7, not 8)
     const WPlan pl = make_wplan(p.B, dtype_size(p.dtype), tma, EMIT, kSingleBuffer);
-    const uint32_t room = c->max_smem_optin > (int)kTableBytes ? (uint32_t)c->max_smem_optin - kTableBytes : 0u;
+    const uint32_t fixed = cta_fixed_bytes(p.B, EMIT);
+    const uint32_t room = c->max_smem_optin > (int)fixed ? (uint32_t)c->max_smem_optin - fixed : 0u;
     W = std::min<uint32_t>(W, std::max<uint32_t>(1, room / pl.bytes));
     switch (p.dtype) {
     case MTX_DTYPE_U8: return EMIT ? run_emit<uint8_t>(c, p, a, map, tma, W, s) : run_count<uint8_t>(c, p, a, map, tma, W, s);

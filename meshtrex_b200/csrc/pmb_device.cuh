@@ -40,12 +40,20 @@ constexpr int kMaxWarps = 8;                        // warps per CTA of the extr
 
 __host__ __device__ inline uint32_t align_up(uint32_t v, uint32_t a) { return (v + a - 1) / a * a; }
 
+// Bytes of a CTA's shared memory before its warps' regions: the case tables,
+// and for the emit pass the context-layer map (ctx_map_entry, one word per
+// voxel of the (B+1)^3 context outside the block).
+__host__ __device__ inline uint32_t cta_fixed_bytes(uint32_t B, bool emit) {
+    return kTableBytes + (emit ? align_up(4 * (3 * B * B + 3 * B + 1), 128) : 0u);
+}
+
 // ------------------------------------------------------- per-warp smem plan
 struct WPlan {
     uint32_t B, B1, BB, PX, nbuf, nb3;
     uint32_t rB, rB1, rBB;  // ceil(2^32 / d) reciprocals: n / d == __umulhi(n, r) for the sizes used here
     uint32_t R;             // block rows walked per round of 32 lanes (32 / B)
     uint32_t off_tile[2], off_bar, off_rows, off_cross, off_vp, off_tp, off_nvid, off_nm, off_jobs;
+    uint32_t off_case, off_mm;  // emit pass: case byte of each mixed cell, mixed-cell mask of each cell row
     uint32_t off_vtab, off_vmsk, off_list;  // balanced bodies only (pmb_balanced.cuh)
     uint32_t bytes;       // per warp
     uint32_t tile_bytes;  // one tile (the TMA transaction size)
@@ -96,6 +104,10 @@ __host__ __device__ inline WPlan make_wplan(uint32_t B, uint32_t esz, bool tma, 
         o = align_up(o + 4 * p.nb3, 16);
         p.off_nm = o;
         o = align_up(o + p.nb3, 16);
+        p.off_case = o;
+        o = align_up(o + B * B * B, 16);
+        p.off_mm = o;
+        o = align_up(o + 2 * B * B, 16);
     }
     p.off_jobs = o;  // a window of packed jobs (triangles or vertices) in output order
     o = align_up(o + 4 * kJobWin, 16);
@@ -339,10 +351,12 @@ __device__ __forceinline__ uint32_t mixed_cells(const Problem &p, const WPlan &p
 // Per-row crossing masks, vertex prefixes and (want_tris) triangle prefixes,
 // and the block's vertex/triangle counts.  Lane l owns rows [l*R, l*R + R) so
 // that the row prefixes follow from one warp scan.  Optionally writes the
-// per-cell case bytes.
+// per-cell case bytes (cases_out: every cell, 0 / 255 for cells that are not
+// mixed) and keeps, in the warp's shared memory, the mixed-cell mask of each
+// cell row and the case byte of each mixed cell (keep: the emit pass).
 __device__ __forceinline__ void block_counts(const Problem &p, const WPlan &pl, unsigned char *ws, const Geo &g,
                                              const uint8_t *ntab, bool want_tris, uint8_t *cases_out,
-                                             uint32_t &nv, uint32_t &nt) {
+                                             uint32_t &nv, uint32_t &nt, bool keep = false) {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t *rows = reinterpret_cast<const uint32_t *>(ws + pl.off_rows);
     uint32_t *cross = reinterpret_cast<uint32_t *>(ws + pl.off_cross);
@@ -368,12 +382,14 @@ __device__ __forceinline__ void block_counts(const Problem &p, const WPlan &pl, 
             uint32_t mm = mixed_cells(p, pl, g, rows, y, z, inside);
             if (cases_out)
                 for (uint32_t x = 0; x < B; ++x) cases_out[q * B + x] = ((inside >> x) & 1u) ? 255 : 0;
+            if (keep) reinterpret_cast<uint16_t *>(ws + pl.off_mm)[q] = (uint16_t)mm;
             while (mm) {
                 const uint32_t x = __ffs(mm) - 1;
                 mm &= mm - 1u;
                 const uint32_t cfg = cell_case(rows, pl.B1, x, y, z);
                 stri += ntab[cfg];
                 if (cases_out) cases_out[q * B + x] = (uint8_t)cfg;
+                if (keep) ws[pl.off_case + q * B + x] = (uint8_t)cfg;
             }
         }
     }
@@ -710,7 +726,9 @@ __device__ __forceinline__ uint32_t neighbour_rank(const Problem &p, const Geo &
 }
 
 // Issues the loads of the face records of the block's +x/+y/+z context layer
-// (all of them before any is used); bit 31 of rec marks a present record.
+// (all of them before any is used); bit 31 of rec marks a present record and
+// bits 27-29 hold the number c of the neighbour it came from (face records
+// use bits 0-26).
 template <int CPL, bool NC = true>
 __device__ __forceinline__ void gather_issue(const Problem &p, const WPlan &pl, const Geo &g, uint32_t nb_rk,
                                              const uint32_t *faces, uint32_t face_stride, uint32_t rec[CPL]) {
@@ -728,8 +746,46 @@ __device__ __forceinline__ void gather_issue(const Problem &p, const WPlan &pl, 
         if (j < nb3 && rk != kNoVertex && g.ox + x < p.X && g.oy + y < p.Y && g.oz + z < p.Z) {
             const uint32_t lx = dx ? 0 : x, ly = dy ? 0 : y, lz = dz ? 0 : z;
             const uint32_t e = dx ? lz * B + ly : (dy ? BB + lz * B + lx : 2 * BB + ly * B + lx);
-            rec[k] = ld_in<NC>(faces + (uint64_t)rk * face_stride + e) | 0x80000000u;
+            rec[k] = ld_in<NC>(faces + (uint64_t)rk * face_stride + e) | 0x80000000u | (c << 27);
         }
+    }
+}
+
+// Map entry of context voxel j: neighbour number c (bits 0-2), the index of its
+// face record in that neighbour (bits 3-12), and the voxel's block coordinates
+// x, y, z (5 bits each from bit 13).  It depends on B alone, so the emit kernel
+// builds the map once per CTA.
+__device__ __forceinline__ uint32_t ctx_map_entry(const WPlan &pl, uint32_t j) {
+    const uint32_t B = pl.B, BB = pl.BB;
+    uint32_t x, y, z;
+    ctx_voxel(pl, j, x, y, z);
+    const uint32_t dx = x == B, dy = y == B, dz = z == B;
+    const uint32_t lx = dx ? 0 : x, ly = dy ? 0 : y, lz = dz ? 0 : z;
+    const uint32_t e = dx ? lz * B + ly : (dy ? BB + lz * B + lx : 2 * BB + ly * B + lx);
+    return (dx | (dy << 1) | (dz << 2)) | (e << 3) | (x << 13) | (y << 18) | (z << 23);
+}
+
+// gather_issue with the context-layer map in shared memory.
+template <int CPL>
+__device__ __forceinline__ void gather_issue_map(const Problem &p, const WPlan &pl, const Geo &g, uint32_t nb_rk,
+                                                 const uint32_t *faces, uint32_t face_stride, const uint32_t *cmap,
+                                                 uint32_t rec[CPL]) {
+    const uint32_t lane = threadIdx.x & 31, nb3 = pl.nb3;
+    // the whole context layer lies in the volume unless the block reaches a high face
+    const bool inner = g.ox + pl.B < p.X && g.oy + pl.B < p.Y && g.oz + pl.B < p.Z;
+#pragma unroll
+    for (uint32_t k = 0; k < CPL; ++k) {
+        rec[k] = 0;
+        if (k * 32 >= nb3) continue;  // warp-uniform
+        const uint32_t j = k * 32 + lane;
+        const uint32_t m = cmap[j < nb3 ? j : 0];
+        const uint32_t c = j < nb3 ? (m & 7u) : 1u;
+        const uint32_t rk = __shfl_sync(0xffffffffu, nb_rk, c);
+        bool take = j < nb3 && rk != kNoVertex;
+        if (!inner)
+            take = take && g.ox + ((m >> 13) & 31u) < p.X && g.oy + ((m >> 18) & 31u) < p.Y &&
+                   g.oz + ((m >> 23) & 31u) < p.Z;
+        if (take) rec[k] = __ldg(faces + (uint64_t)rk * face_stride + ((m >> 3) & 1023u)) | 0x80000000u | (c << 27);
     }
 }
 
@@ -738,17 +794,14 @@ __device__ __forceinline__ void gather_issue(const Problem &p, const WPlan &pl, 
 template <int CPL>
 __device__ __forceinline__ void gather_finish(const WPlan &pl, uint32_t nb_vb, const uint32_t rec[CPL],
                                               unsigned char *ws) {
-    const uint32_t lane = threadIdx.x & 31, B = pl.B, nb3 = pl.nb3;
+    const uint32_t lane = threadIdx.x & 31, nb3 = pl.nb3;
     uint32_t *nvid = reinterpret_cast<uint32_t *>(ws + pl.off_nvid);
     uint8_t *nm = ws + pl.off_nm;
 #pragma unroll
     for (uint32_t k = 0; k < CPL; ++k) {
         if (k * 32 >= nb3) continue;
         const uint32_t j = k * 32 + lane;
-        uint32_t x, y, z;
-        ctx_voxel(pl, j < nb3 ? j : 0, x, y, z);
-        const uint32_t c = j < nb3 ? ((x == B) | ((y == B) << 1) | ((z == B) << 2)) : 1u;
-        const uint32_t vb = __shfl_sync(0xffffffffu, nb_vb, c);
+        const uint32_t vb = __shfl_sync(0xffffffffu, nb_vb, (rec[k] >> 27) & 7u);
         if (j < nb3) {
             const bool present = rec[k] >> 31;
             nvid[j] = present ? vb + (rec[k] & 0xffffffu) : kNoVertex;
@@ -789,8 +842,7 @@ __device__ __forceinline__ void emit_block(const Problem &p, const WPlan &pl, un
                                            const uint8_t *ntab, const uint8_t *owner, uint32_t *indices,
                                            uint64_t tcap, void *vertices, uint64_t vcap, uint32_t vfmt,
                                            uint32_t frame, uint32_t normals, DevStatus *st, uint32_t r) {
-    const uint32_t lane = threadIdx.x & 31, B = pl.B, BB = pl.BB, B1 = pl.B1;
-    const uint32_t *rows = reinterpret_cast<const uint32_t *>(ws + pl.off_rows);
+    const uint32_t lane = threadIdx.x & 31, B = pl.B, BB = pl.BB;
     const uint32_t *cross = reinterpret_cast<const uint32_t *>(ws + pl.off_cross);
     const uint32_t *vp = reinterpret_cast<const uint32_t *>(ws + pl.off_vp);
     const uint32_t *tp = reinterpret_cast<const uint32_t *>(ws + pl.off_tp);
@@ -805,15 +857,17 @@ __device__ __forceinline__ void emit_block(const Problem &p, const WPlan &pl, un
     if (!(d.primitiveCount || (vertices && d.vertexCount))) return;
     build_rows<T>(p, pl, ws, buf, g);
     uint32_t bnv, bnt;
-    block_counts(p, pl, ws, g, ntab, true, nullptr, bnv, bnt);
+    block_counts(p, pl, ws, g, ntab, true, nullptr, bnv, bnt, true);
     if (lane == 0 && (bnv != d.vertexCount || bnt != d.primitiveCount))
         report(st, MTX_ERR_INTERNAL, kSiteEmitNeighbour, r, 2);
     if (vertices && bnv)
         emit_vertices<T, GENERIC, ANY>(p, pl, ws, buf, g, d.vertexOffset, bnv, vertices, vfmt, frame, normals);
     // triangles in canonical order: each lane walks the mixed cells of its rows
-    // and writes one job per triangle (cell | t << 12 | case << 16) at the
-    // triangle's own position in a window of kJobWin jobs; the warp resolves
-    // 32 triangles at a time
+    // (masks and case bytes kept by block_counts) and writes one job per
+    // triangle (cell | t << 12 | case << 16) at the triangle's own position in
+    // a window of kJobWin jobs; the warp resolves 32 triangles at a time
+    const uint16_t *mmk = reinterpret_cast<const uint16_t *>(ws + pl.off_mm);
+    const uint8_t *ck = ws + pl.off_case;
     const uint32_t R = (BB + 31) / 32, nt = d.primitiveCount;
     bool bad = false;
     for (uint32_t w0 = 0; w0 < nt; w0 += kJobWin) {
@@ -824,13 +878,11 @@ __device__ __forceinline__ void emit_block(const Problem &p, const WPlan &pl, un
             uint32_t j = tp[q];
             const uint32_t jend = (q + 1 < BB) ? tp[q + 1] : nt;
             if (j >= w1 || jend <= w0) continue;
-            const uint32_t z = fdiv(q, pl.rB), y = q - z * B;
-            uint32_t inside;
-            uint32_t mm = mixed_cells(p, pl, g, rows, y, z, inside);
+            uint32_t mm = mmk[q];
             while (mm) {
                 const uint32_t x = __ffs(mm) - 1;
                 mm &= mm - 1u;
-                const uint32_t cfg = cell_case(rows, B1, x, y, z);
+                const uint32_t cfg = ck[q * B + x];
                 const uint32_t n = ntab[cfg];
                 for (uint32_t t = 0; t < n; ++t, ++j)
                     if (j >= w0 && j < w1) jobs[j - w0] = (q * B + x) | (t << 12) | (cfg << 16);
