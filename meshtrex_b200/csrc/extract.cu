@@ -169,8 +169,8 @@ __global__ void __launch_bounds__(kMaxWarps * 32, (!GENERIC && CPL == 8) ? 3 : 1
             break;
         }
         gather_finish<CPL>(pl, nb_vb, rec, ws);
-        emit_block<T, GENERIC>(p, pl, ws, buf, g, d, tab, ntab, owner, indices, tcap, vertices, vcap, vfmt, frame,
-                               normals, st, r);
+        emit_block<T, GENERIC, false, CPL == 8>(p, pl, ws, buf, g, d, tab, ntab, owner, indices, tcap, vertices,
+                                                vcap, vfmt, frame, normals, st, r);
         if (!have_next) break;
         if (pl.nbuf == 1) tile_issue<T, TMA>(pl, ws, buf, gn, &map);
         else buf ^= 1u;

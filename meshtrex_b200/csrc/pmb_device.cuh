@@ -83,10 +83,12 @@ __host__ __device__ inline WPlan make_wplan(uint32_t B, uint32_t esz, bool tma, 
     p.PX = tile_pitch(B, esz, tma);
     p.tile_bytes = p.PX * p.B1 * p.B1 * esz;
     p.nbuf = (p.tile_bytes <= 4096 && !single_buffer) ? 2 : 1;
+    // the emit pass puts its voxel table (build_vtab, B <= 8) in the tile's slot
+    const uint32_t slot = (tri_pass && B <= 8) ? std::max(p.tile_bytes, 2 * B * B * B) : p.tile_bytes;
     uint32_t o = 0;
     for (uint32_t b = 0; b < 2; ++b) {
         p.off_tile[b] = o;
-        if (b < p.nbuf) o = align_up(o + p.tile_bytes, 128);
+        if (b < p.nbuf) o = align_up(o + slot, 128);
     }
     if (p.nbuf == 1) p.off_tile[1] = p.off_tile[0];
     p.off_bar = o;
@@ -633,6 +635,55 @@ __device__ __forceinline__ uint32_t edge_vertex(uint32_t x, uint32_t y, uint32_t
     return base + __popc(m & ((1u << ax) - 1u));
 }
 
+// Voxel table of the block's own voxels for B <= 8, built in the tile's slot
+// once the vertices are written: entry (z*B + y)*B + x holds the voxel's first
+// vertex relative to the block (11 bits: at most 3 * 512) and its owned-edge
+// mask << 11.  Only voxels that own a cut edge are written; triangle corners
+// refer to no other.
+__device__ __forceinline__ void build_vtab(const WPlan &pl, const unsigned char *ws, uint16_t *vt) {
+    const uint32_t lane = threadIdx.x & 31, B = pl.B, BB = pl.BB, R = (BB + 31) / 32;
+    const uint32_t *cross = reinterpret_cast<const uint32_t *>(ws + pl.off_cross);
+    const uint32_t *vp = reinterpret_cast<const uint32_t *>(ws + pl.off_vp);
+    for (uint32_t k = 0; k < R; ++k) {
+        const uint32_t q = lane * R + k;
+        if (q >= BB) break;
+        const uint32_t xc = cross[q], yc = cross[BB + q], zc = cross[2 * BB + q];
+        uint32_t any = xc | yc | zc, run = vp[q];
+        while (any) {
+            const uint32_t x = __ffs(any) - 1;
+            any &= any - 1u;
+            const uint32_t m = ((xc >> x) & 1u) | (((yc >> x) & 1u) << 1) | (((zc >> x) & 1u) << 2);
+            vt[q * B + x] = (uint16_t)(run | (m << 11));
+            run += __popc(m);
+        }
+    }
+    __syncwarp();
+}
+
+// edge_vertex with the block's own voxels looked up in the voxel table.
+__device__ __forceinline__ uint32_t edge_vertex_vt(uint32_t x, uint32_t y, uint32_t z, uint32_t e,
+                                                   const uint8_t *owner, const uint16_t *vt, const uint32_t *nvid,
+                                                   const uint8_t *nm, uint32_t B, uint32_t vbase, bool &bad) {
+    const uint32_t own = owner[e];
+    const uint32_t ux = x + (own & 1u), uy = y + ((own >> 1) & 1u), uz = z + ((own >> 2) & 1u);
+    const uint32_t ax = own >> 3;
+    uint32_t base, m;
+    if (ux < B && uy < B && uz < B) {
+        const uint32_t v = vt[(uz * B + uy) * B + ux];
+        base = vbase + (v & 0x7ffu);
+        m = v >> 11;
+    } else {
+        const uint32_t jx = ctx_index(B, ux, uy, uz);
+        base = nvid[jx];
+        m = nm[jx];
+    }
+    if (base == kNoVertex || !((m >> ax) & 1u)) {
+        bad = true;
+        return 0;
+    }
+    return base + __popc(m & ((1u << ax) - 1u));
+}
+
 // -------------------------------------------------------------- scan pass
 constexpr uint64_t kCnt31 = 0x7fffffffull;
 
@@ -835,8 +886,9 @@ __device__ __forceinline__ void count_block(const Problem &p, const WPlan &pl, u
 
 // Emit body of one block whose tile is staged and whose context layer has
 // been gathered: its own vertices (when `vertices` is set) and its triangles.
-// ANY as in emit_vertices.
-template <typename T, bool GENERIC, bool ANY = false>
+// ANY as in emit_vertices.  VT: resolve triangle corners through the voxel
+// table (build_vtab; B <= 8 only).
+template <typename T, bool GENERIC, bool ANY = false, bool VT = false>
 __device__ __forceinline__ void emit_block(const Problem &p, const WPlan &pl, unsigned char *ws, uint32_t buf,
                                            const Geo &g, const mtx_meshlet_descriptor &d, const uint64_t *tab,
                                            const uint8_t *ntab, const uint8_t *owner, uint32_t *indices,
@@ -868,6 +920,8 @@ __device__ __forceinline__ void emit_block(const Problem &p, const WPlan &pl, un
     // a window of kJobWin jobs; the warp resolves 32 triangles at a time
     const uint16_t *mmk = reinterpret_cast<const uint16_t *>(ws + pl.off_mm);
     const uint8_t *ck = ws + pl.off_case;
+    uint16_t *vt = reinterpret_cast<uint16_t *>(ws + pl.off_tile[buf]);  // the tile is dead past the vertices
+    if constexpr (VT) build_vtab(pl, ws, vt);
     const uint32_t R = (BB + 31) / 32, nt = d.primitiveCount;
     bool bad = false;
     for (uint32_t w0 = 0; w0 < nt; w0 += kJobWin) {
@@ -899,12 +953,20 @@ __device__ __forceinline__ void emit_block(const Problem &p, const WPlan &pl, un
                 const uint32_t z = fdiv(q, pl.rB), y = q - z * B;
                 const uint64_t w = tab[job >> 16] >> (4 + 12 * t);
                 uint32_t *o = indices + 3ull * (tbase + w0 + b + lane);  // each lane its own 12 bytes
-                o[0] = edge_vertex(x, y, z, (uint32_t)(w & 0xFu), owner, cross, vp, nvid, nm, B, BB, d.vertexOffset,
-                                   bad);
-                o[1] = edge_vertex(x, y, z, (uint32_t)((w >> 4) & 0xFu), owner, cross, vp, nvid, nm, B, BB,
-                                   d.vertexOffset, bad);
-                o[2] = edge_vertex(x, y, z, (uint32_t)((w >> 8) & 0xFu), owner, cross, vp, nvid, nm, B, BB,
-                                   d.vertexOffset, bad);
+                if constexpr (VT) {
+                    o[0] = edge_vertex_vt(x, y, z, (uint32_t)(w & 0xFu), owner, vt, nvid, nm, B, d.vertexOffset, bad);
+                    o[1] = edge_vertex_vt(x, y, z, (uint32_t)((w >> 4) & 0xFu), owner, vt, nvid, nm, B,
+                                          d.vertexOffset, bad);
+                    o[2] = edge_vertex_vt(x, y, z, (uint32_t)((w >> 8) & 0xFu), owner, vt, nvid, nm, B,
+                                          d.vertexOffset, bad);
+                } else {
+                    o[0] = edge_vertex(x, y, z, (uint32_t)(w & 0xFu), owner, cross, vp, nvid, nm, B, BB,
+                                       d.vertexOffset, bad);
+                    o[1] = edge_vertex(x, y, z, (uint32_t)((w >> 4) & 0xFu), owner, cross, vp, nvid, nm, B, BB,
+                                       d.vertexOffset, bad);
+                    o[2] = edge_vertex(x, y, z, (uint32_t)((w >> 8) & 0xFu), owner, cross, vp, nvid, nm, B, BB,
+                                       d.vertexOffset, bad);
+                }
             }
             __syncwarp();
         }
