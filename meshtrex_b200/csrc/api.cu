@@ -376,8 +376,8 @@ mtx_status mtx_context_destroy(mtx_context_t c) {
     if (!c) return MTX_ERR_INVALID_ARG;
     DeviceGuard g(c->device);
     cudaStreamSynchronize(c->stream);
-    for (Scratch *s : {&c->filter_status, &c->count_status, &c->faces, &c->leaf, &c->ids, &c->rank, &c->desc, &c->misc,
-                       &c->adj_partial, &c->adj_iso})
+    for (Scratch *s : {&c->filter_status, &c->count_status, &c->faces, &c->state, &c->leaf, &c->ids, &c->rank,
+                       &c->desc, &c->misc, &c->adj_partial, &c->adj_iso})
         dev_free(s->ptr);
     dev_cache_release(c->device);
     cudaFree(c->ctrl);
@@ -633,6 +633,8 @@ mtx_status mtx_extract_meshlet_descriptors(mtx_context_t c, const mtx_minmax_out
         return s;
     };
     if ((r = scratch_reserve(c, c->faces, (size_t)n * 3 * B * B * 4)) != MTX_OK) return bail(r);
+    const uint32_t sb = block_state_bytes(B);
+    if (sb && (r = scratch_reserve(c, c->state, (size_t)n * sb)) != MTX_OK) return bail(r);
 
     ExtractArgs a;
     memset(&a, 0, sizeof(a));
@@ -644,6 +646,7 @@ mtx_status mtx_extract_meshlet_descriptors(mtx_context_t c, const mtx_minmax_out
     a.desc_capacity = n;
     a.block_capacity = n;
     a.faces = (uint32_t *)c->faces.ptr;
+    a.state = sb ? (uint8_t *)c->state.ptr : nullptr;
     a.count_status = (uint64_t *)c->count_status.ptr;
     a.totals = (uint32_t *)counters;
     a.cell_cases = o.cellCases;
@@ -727,6 +730,8 @@ mtx_status mtx_extract_plain_async(mtx_context_t c, const mtx_volume *vol, const
     if ((r = scratch_reserve(c, c->ids, p.nblocks * 4)) != MTX_OK) return r;
     if ((r = scratch_reserve(c, c->rank, p.nblocks * 4)) != MTX_OK) return r;
     if ((r = scratch_reserve(c, c->faces, maxa * 3 * B * B * 4)) != MTX_OK) return r;
+    const uint32_t sb = block_state_bytes(B);
+    if (sb && (r = scratch_reserve(c, c->state, maxa * sb)) != MTX_OK) return r;
     mtx_meshlet_descriptor *desc = out->meshlets;
     uint64_t dcap = out->meshletCapacity;
     if (!desc || dcap < maxa) {
@@ -761,6 +766,7 @@ mtx_status mtx_extract_plain_async(mtx_context_t c, const mtx_volume *vol, const
     a.desc_capacity = dcap;
     a.block_capacity = maxa;
     a.faces = (uint32_t *)c->faces.ptr;
+    a.state = sb ? (uint8_t *)c->state.ptr : nullptr;
     a.count_status = (uint64_t *)c->count_status.ptr;
     a.totals = out->counters;
     a.cell_cases = o.cellCases;

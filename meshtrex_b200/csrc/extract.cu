@@ -28,10 +28,10 @@ template <typename T, bool TMA>
 __global__ void __launch_bounds__(kMaxWarps * 32)
     pmb_count_kernel(Problem p, const __grid_constant__ CUtensorMap map, const uint32_t *__restrict__ ids,
                      const uint32_t *__restrict__ count_ptr, mtx_meshlet_descriptor *__restrict__ desc,
-                     uint64_t desc_cap, uint32_t *__restrict__ faces, uint32_t *totals,
-                     uint8_t *__restrict__ cell_cases, uint64_t block_cap, DevStatus *st) {
+                     uint64_t desc_cap, uint32_t *__restrict__ faces, uint8_t *__restrict__ state,
+                     uint32_t *totals, uint8_t *__restrict__ cell_cases, uint64_t block_cap, DevStatus *st) {
     extern __shared__ __align__(128) unsigned char smem[];
-    const WPlan pl = make_wplan(p.B, sizeof(T), TMA, false, kSingleBuffer);
+    const WPlan pl = make_wplan(p.B, sizeof(T), TMA, false, kSingleBuffer, p.B <= 8);
     uint8_t *ntab = smem + 2048;
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, W = blockDim.x >> 5;
     unsigned char *ws = smem + kTableBytes + warp * pl.bytes;
@@ -74,7 +74,8 @@ __global__ void __launch_bounds__(kMaxWarps * 32)
             break;
         }
         count_block<T>(p, pl, ws, buf, g, ntab, cell_cases ? cell_cases + (uint64_t)r * B3 : nullptr, desc + r,
-                       faces + (uint64_t)r * 3 * pl.BB);
+                       faces + (uint64_t)r * 3 * pl.BB,
+                       (state && pl.state_bytes) ? state + (uint64_t)r * pl.state_bytes : nullptr);
         if (!have_next) break;
         if (pl.nbuf == 1) tile_issue<T, TMA>(pl, ws, buf, gn, &map);
         else buf ^= 1u;
@@ -108,8 +109,11 @@ __global__ void __launch_bounds__(kMaxWarps * 32, (!GENERIC && CPL == 8) ? 3 : 1
     pmb_emit_kernel(Problem p, const __grid_constant__ CUtensorMap map, const uint32_t *__restrict__ ids,
                     const uint32_t *__restrict__ rank_map, const uint32_t *__restrict__ count_ptr,
                     const mtx_meshlet_descriptor *__restrict__ desc, const uint32_t *__restrict__ faces,
-                    uint32_t *__restrict__ indices, uint64_t tcap, uint64_t block_cap, void *__restrict__ vertices,
-                    uint64_t vcap, uint32_t vfmt, uint32_t frame, uint32_t normals, DevStatus *st) {
+                    const uint8_t *__restrict__ state, uint32_t *__restrict__ indices, uint64_t tcap,
+                    uint64_t block_cap, void *__restrict__ vertices, uint64_t vcap, uint32_t vfmt, uint32_t frame,
+                    uint32_t normals, DevStatus *st) {
+    // B <= 8 with TMA: the count pass's block state comes with each tile
+    constexpr bool STATE = TMA && CPL == 8;
     extern __shared__ __align__(128) unsigned char smem[];
     const WPlan pl = make_wplan(p.B, sizeof(T), TMA, true, kSingleBuffer);
     uint64_t *tab = reinterpret_cast<uint64_t *>(smem);
@@ -140,10 +144,13 @@ __global__ void __launch_bounds__(kMaxWarps * 32, (!GENERIC && CPL == 8) ? 3 : 1
     Geo g{};
     mtx_meshlet_descriptor d{};
     uint32_t nb_rk = kNoVertex;
+    auto state_of = [&](uint32_t rr) -> const unsigned char * {
+        return STATE ? state + (uint64_t)rr * pl.state_bytes : nullptr;
+    };
     if (r < count) {
         const uint32_t id = __ldg(ids + r);
         g = block_geo(id, p, TMA, sizeof(T));
-        tile_issue<T, TMA>(pl, ws, buf, g, &map);
+        tile_issue<T, TMA>(pl, ws, buf, g, &map, state_of(r));
         d = desc[r];
         nb_rk = neighbour_rank(p, g, id, rank_map);
     }
@@ -157,7 +164,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32, (!GENERIC && CPL == 8) ? 3 : 1
         if (have_next) {
             const uint32_t idn = __ldg(ids + rn);
             gn = block_geo(idn, p, TMA, sizeof(T));
-            if (pl.nbuf == 2) tile_issue<T, TMA>(pl, ws, buf ^ 1u, gn, &map);
+            if (pl.nbuf == 2) tile_issue<T, TMA>(pl, ws, buf ^ 1u, gn, &map, state_of(rn));
             dn = desc[rn];
             nb_rk_n = neighbour_rank(p, gn, idn, rank_map);
         }
@@ -169,10 +176,10 @@ __global__ void __launch_bounds__(kMaxWarps * 32, (!GENERIC && CPL == 8) ? 3 : 1
             break;
         }
         gather_finish<CPL>(pl, nb_vb, rec, ws);
-        emit_block<T, GENERIC, false, CPL == 8>(p, pl, ws, buf, g, d, tab, ntab, owner, indices, tcap, vertices,
-                                                vcap, vfmt, frame, normals, st, r);
+        emit_block<T, GENERIC, false, CPL == 8, STATE>(p, pl, ws, buf, g, d, tab, ntab, owner, indices, tcap,
+                                                       vertices, vcap, vfmt, frame, normals, st, r);
         if (!have_next) break;
-        if (pl.nbuf == 1) tile_issue<T, TMA>(pl, ws, buf, gn, &map);
+        if (pl.nbuf == 1) tile_issue<T, TMA>(pl, ws, buf, gn, &map, state_of(rn));
         else buf ^= 1u;
         r = rn;
         d = dn;
@@ -209,14 +216,14 @@ static mtx_status grid_for(mtx_context *c, K kernel, int threads, uint32_t smem,
 template <typename T>
 static mtx_status run_count(mtx_context *c, const Problem &p, const ExtractArgs &a, const CUtensorMap &map, bool tma,
                             uint32_t W, cudaStream_t s) {
-    const WPlan pl = make_wplan(p.B, sizeof(T), tma, false, kSingleBuffer);
+    const WPlan pl = make_wplan(p.B, sizeof(T), tma, false, kSingleBuffer, p.B <= 8);
     const uint32_t smem = kTableBytes + W * pl.bytes;
     auto k = tma ? pmb_count_kernel<T, true> : pmb_count_kernel<T, false>;
     unsigned grid;
     mtx_status r = grid_for(c, k, W * 32, smem, a.host_count, W, grid);
     if (r != MTX_OK) return r;
-    k<<<grid, W * 32, smem, s>>>(p, map, a.ids, a.count, a.desc, a.desc_capacity, a.faces, a.totals, a.cell_cases,
-                                 a.block_capacity, &c->ctrl->status);
+    k<<<grid, W * 32, smem, s>>>(p, map, a.ids, a.count, a.desc, a.desc_capacity, a.faces, a.state, a.totals,
+                                 a.cell_cases, a.block_capacity, &c->ctrl->status);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "count launch");
     return MTX_OK;
@@ -224,8 +231,8 @@ static mtx_status run_count(mtx_context *c, const Problem &p, const ExtractArgs 
 
 template <typename T, int CPL, bool TMA>
 static void (*emit_fn(bool generic))(Problem, CUtensorMap, const uint32_t *, const uint32_t *, const uint32_t *,
-                                     const mtx_meshlet_descriptor *, const uint32_t *, uint32_t *, uint64_t, uint64_t,
-                                     void *, uint64_t, uint32_t, uint32_t, uint32_t, DevStatus *) {
+                                     const mtx_meshlet_descriptor *, const uint32_t *, const uint8_t *, uint32_t *,
+                                     uint64_t, uint64_t, void *, uint64_t, uint32_t, uint32_t, uint32_t, DevStatus *) {
     return generic ? pmb_emit_kernel<T, CPL, TMA, true> : pmb_emit_kernel<T, CPL, TMA, false>;
 }
 
@@ -240,9 +247,9 @@ static mtx_status run_emit(mtx_context *c, const Problem &p, const ExtractArgs &
     unsigned grid;
     mtx_status r = grid_for(c, k, W * 32, smem, a.host_count, W, grid);
     if (r != MTX_OK) return r;
-    k<<<grid, W * 32, smem, s>>>(p, map, a.ids, a.rank_map, a.count, a.desc, a.faces, a.indices, a.tri_capacity,
-                                 a.block_capacity, a.vertices, a.vertex_capacity, a.vertex_format, a.frame, a.normals,
-                                 &c->ctrl->status);
+    k<<<grid, W * 32, smem, s>>>(p, map, a.ids, a.rank_map, a.count, a.desc, a.faces, a.state, a.indices,
+                                 a.tri_capacity, a.block_capacity, a.vertices, a.vertex_capacity, a.vertex_format,
+                                 a.frame, a.normals, &c->ctrl->status);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "emit launch");
     return MTX_OK;
@@ -265,7 +272,9 @@ static mtx_status launch_stage(mtx_context *c, const Problem &p, const ExtractAr
     uint32_t W = a.threads ? a.threads / 32 : (c->tuning.extractWarps ? c->tuning.extractWarps : 4);
     W = std::min<uint32_t>(std::max<uint32_t>(W, 1), kMaxWarps);
     // no more warps than the shared memory holds (16^3 float tiles fit 7, not 8)
-    const WPlan pl = make_wplan(p.B, dtype_size(p.dtype), tma, EMIT, kSingleBuffer);
+    const WPlan pl = make_wplan(p.B, dtype_size(p.dtype), tma, EMIT, kSingleBuffer, p.B <= 8);
+    // the emit pass with TMA and B <= 8 reads the block state the count pass wrote
+    if (EMIT && tma && pl.state_bytes && !a.state) return fail(c, MTX_ERR_INTERNAL, "emit without block state");
     const uint32_t fixed = cta_fixed_bytes(p.B, EMIT);
     const uint32_t room = c->max_smem_optin > (int)fixed ? (uint32_t)c->max_smem_optin - fixed : 0u;
     W = std::min<uint32_t>(W, std::max<uint32_t>(1, room / pl.bytes));
@@ -275,6 +284,8 @@ static mtx_status launch_stage(mtx_context *c, const Problem &p, const ExtractAr
     default: return EMIT ? run_emit<float>(c, p, a, map, tma, W, s) : run_count<float>(c, p, a, map, tma, W, s);
     }
 }
+
+uint32_t block_state_bytes(uint32_t B) { return make_wplan(B, 2, true, false, kSingleBuffer, B <= 8).state_bytes; }
 
 // Counts, faces and the scan: after this the descriptors and totals are final.
 mtx_status launch_count(mtx_context *c, const Problem &p, const ExtractArgs &a, cudaStream_t s) {

@@ -44,7 +44,7 @@ struct mtx_context {
     uint32_t fail_alloc_in = 0;  // fault injection: fail the k-th allocation
     mtx::Ctrl *ctrl = nullptr;   // device
     uint32_t *pinned = nullptr;  // pinned host words for count readbacks
-    mtx::Scratch filter_status, count_status, faces, leaf, ids, rank, desc, misc;
+    mtx::Scratch filter_status, count_status, faces, state, leaf, ids, rank, desc, misc;
     mtx::Scratch adj_partial, adj_iso;  // adjoint: per-block partial tiles and isovalue sums
     mtx_profiler *prof = nullptr;  // records stage times of calls given no profiler
     mtx_tuning tuning = {0, 0, 0, 0};
@@ -133,6 +133,7 @@ struct ExtractArgs {
     mtx_meshlet_descriptor *desc;  // per active block {vbase, 3*tbase, nv, nt}
     uint64_t desc_capacity;
     uint32_t *faces;            // 3*B*B words per active block
+    uint8_t *state;             // block_state_bytes(B) per active block (count -> emit), B <= 8
     uint64_t block_capacity;    // active blocks that desc/faces/count_status can hold
     uint64_t *count_status;     // unused (the scan keeps its own look-back words)
     uint32_t *totals;           // device uint32[4] {vertexCount, indexCount, meshletCount, activeCount}
@@ -144,6 +145,8 @@ struct ExtractArgs {
     uint32_t vertex_format, frame, normals, staging, threads;
 };
 mtx_status launch_count(mtx_context *c, const Problem &p, const ExtractArgs &a, cudaStream_t s);
+// Bytes of the block state the count pass hands to the emit pass (0: none, B > 8).
+uint32_t block_state_bytes(uint32_t B);
 // The descriptor scan alone over *count descriptors (capacity bounds them).
 mtx_status launch_desc_scan(mtx_context *c, mtx_meshlet_descriptor *desc, const uint32_t *count, uint64_t capacity,
                             uint32_t *totals, cudaStream_t s);

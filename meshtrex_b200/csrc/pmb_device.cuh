@@ -53,7 +53,8 @@ struct WPlan {
     uint32_t rB, rB1, rBB;  // ceil(2^32 / d) reciprocals: n / d == __umulhi(n, r) for the sizes used here
     uint32_t R;             // block rows walked per round of 32 lanes (32 / B)
     uint32_t off_tile[2], off_bar, off_rows, off_cross, off_vp, off_tp, off_nvid, off_nm, off_jobs;
-    uint32_t off_case, off_mm;  // emit pass: case byte of each mixed cell, mixed-cell mask of each cell row
+    uint32_t off_case, off_mm;  // case byte of each mixed cell, mixed-cell mask of each cell row (kept)
+    uint32_t state_bytes;       // block state handed from count to emit (B <= 8): [off_cross, off_mm + 2BB)
     uint32_t off_vtab, off_vmsk, off_list;  // balanced bodies only (pmb_balanced.cuh)
     uint32_t bytes;       // per warp
     uint32_t tile_bytes;  // one tile (the TMA transaction size)
@@ -69,8 +70,12 @@ __host__ __device__ inline uint32_t tile_pitch(uint32_t B, uint32_t esz, bool tm
     return align_up(xoff_max + B + 1, A);
 }
 
+// tri_pass: the emit pass's plan.  keep: room for the case bytes and mixed
+// masks (always in the emit pass); for B <= 8 the count pass keeps them too
+// and hands the block state -- crossing rows, row prefixes, case bytes and
+// mixed masks, one contiguous range -- to the emit pass through global memory.
 __host__ __device__ inline WPlan make_wplan(uint32_t B, uint32_t esz, bool tma, bool tri_pass,
-                                            bool single_buffer = false) {
+                                            bool single_buffer = false, bool keep = false) {
     WPlan p{};
     p.B = B;
     p.B1 = B + 1;
@@ -101,15 +106,18 @@ __host__ __device__ inline WPlan make_wplan(uint32_t B, uint32_t esz, bool tma, 
     o = align_up(o + 4 * p.BB, 16);
     p.off_tp = o;
     o = align_up(o + 4 * p.BB, 16);
+    if (tri_pass || keep) {
+        p.off_case = o;
+        o = align_up(o + B * B * B, 16);
+        p.off_mm = o;
+        o = align_up(o + 2 * B * B, 16);
+        p.state_bytes = B <= 8 ? o - p.off_cross : 0u;
+    }
     if (tri_pass) {
         p.off_nvid = o;
         o = align_up(o + 4 * p.nb3, 16);
         p.off_nm = o;
         o = align_up(o + p.nb3, 16);
-        p.off_case = o;
-        o = align_up(o + B * B * B, 16);
-        p.off_mm = o;
-        o = align_up(o + 2 * B * B, 16);
     }
     p.off_jobs = o;  // a window of packed jobs (triangles or vertices) in output order
     o = align_up(o + 4 * kJobWin, 16);
@@ -145,16 +153,19 @@ __device__ __forceinline__ Geo block_geo(uint32_t id, const Problem &p, bool tma
 // Starts the load of a block's (B+1)^3 tile into buffer `buf`.  TMA: lane 0
 // issues one cp.async.bulk.tensor (zero fill outside the volume).  Plain
 // loads are done in tile_wait instead.
+// state: also bring the block's state (pl.state_bytes from global memory)
+// into [off_cross, ...) on the same barrier (TMA only).
 template <typename T, bool TMA>
 __device__ __forceinline__ void tile_issue(const WPlan &pl, unsigned char *ws, uint32_t buf, const Geo &g,
-                                           const CUtensorMap *map) {
+                                           const CUtensorMap *map, const unsigned char *state = nullptr) {
     if (!TMA) return;
     __syncwarp();
     if ((threadIdx.x & 31) == 0) {
         uint64_t *bar = reinterpret_cast<uint64_t *>(ws + pl.off_bar) + buf;
         fence_proxy_async();  // earlier generic reads of this buffer come first
-        mbar_arrive_expect_tx(bar, pl.tile_bytes);
+        mbar_arrive_expect_tx(bar, pl.tile_bytes + (state ? pl.state_bytes : 0u));
         tma_load_3d(ws + pl.off_tile[buf], map, bar, (int)(g.ox - g.xoff), (int)g.oy, (int)g.oz);
+        if (state) bulk_load(ws + pl.off_cross, state, pl.state_bytes, bar);
     }
 }
 
@@ -868,14 +879,19 @@ __device__ __forceinline__ void gather_finish(const WPlan &pl, uint32_t nb_vb, c
 template <typename T>
 __device__ __forceinline__ void count_block(const Problem &p, const WPlan &pl, unsigned char *ws, uint32_t buf,
                                             const Geo &g, const uint8_t *ntab, uint8_t *cases_out,
-                                            mtx_meshlet_descriptor *dr, uint32_t *fr) {
+                                            mtx_meshlet_descriptor *dr, uint32_t *fr, uint8_t *state) {
     const uint32_t lane = threadIdx.x & 31, B = pl.B, BB = pl.BB;
     const uint32_t *cross = reinterpret_cast<const uint32_t *>(ws + pl.off_cross);
     const uint32_t *vp = reinterpret_cast<const uint32_t *>(ws + pl.off_vp);
     build_rows<T>(p, pl, ws, buf, g);
     uint32_t bnv, bnt;
-    block_counts(p, pl, ws, g, ntab, true, cases_out, bnv, bnt);
+    block_counts(p, pl, ws, g, ntab, true, cases_out, bnv, bnt, state != nullptr);
     if (lane == 0) *reinterpret_cast<uint2 *>(&dr->vertexCount) = make_uint2(bnv, bnt);
+    if (state) {  // the block state for the emit pass: 16-byte words, coalesced
+        const uint4 *src = reinterpret_cast<const uint4 *>(ws + pl.off_cross);
+        uint4 *dst = reinterpret_cast<uint4 *>(state);
+        for (uint32_t i = lane; i < pl.state_bytes / 16; i += 32) dst[i] = src[i];
+    }
     for (uint32_t e = lane; e < 3 * BB; e += 32) {
         const uint32_t f = fdiv(e, pl.rBB), i = e - f * BB, b = fdiv(i, pl.rB), a = i - b * B;
         const uint32_t x = f == 0 ? 0 : a, y = f == 0 ? a : (f == 1 ? 0 : b), z = f == 2 ? 0 : b;
@@ -887,8 +903,9 @@ __device__ __forceinline__ void count_block(const Problem &p, const WPlan &pl, u
 // Emit body of one block whose tile is staged and whose context layer has
 // been gathered: its own vertices (when `vertices` is set) and its triangles.
 // ANY as in emit_vertices.  VT: resolve triangle corners through the voxel
-// table (build_vtab; B <= 8 only).
-template <typename T, bool GENERIC, bool ANY = false, bool VT = false>
+// table (build_vtab; B <= 8 only).  STATE: the count pass's block state came
+// with the tile (tile_issue), so the rows and counts are not rebuilt.
+template <typename T, bool GENERIC, bool ANY = false, bool VT = false, bool STATE = false>
 __device__ __forceinline__ void emit_block(const Problem &p, const WPlan &pl, unsigned char *ws, uint32_t buf,
                                            const Geo &g, const mtx_meshlet_descriptor &d, const uint64_t *tab,
                                            const uint8_t *ntab, const uint8_t *owner, uint32_t *indices,
@@ -907,11 +924,14 @@ __device__ __forceinline__ void emit_block(const Problem &p, const WPlan &pl, un
         return;
     }
     if (!(d.primitiveCount || (vertices && d.vertexCount))) return;
-    build_rows<T>(p, pl, ws, buf, g);
-    uint32_t bnv, bnt;
-    block_counts(p, pl, ws, g, ntab, true, nullptr, bnv, bnt, true);
-    if (lane == 0 && (bnv != d.vertexCount || bnt != d.primitiveCount))
-        report(st, MTX_ERR_INTERNAL, kSiteEmitNeighbour, r, 2);
+    uint32_t bnv = d.vertexCount;
+    if constexpr (!STATE) {
+        uint32_t bnt;
+        build_rows<T>(p, pl, ws, buf, g);
+        block_counts(p, pl, ws, g, ntab, true, nullptr, bnv, bnt, true);
+        if (lane == 0 && (bnv != d.vertexCount || bnt != d.primitiveCount))
+            report(st, MTX_ERR_INTERNAL, kSiteEmitNeighbour, r, 2);
+    }
     if (vertices && bnv)
         emit_vertices<T, GENERIC, ANY>(p, pl, ws, buf, g, d.vertexOffset, bnv, vertices, vfmt, frame, normals);
     // triangles in canonical order: each lane walks the mixed cells of its rows
