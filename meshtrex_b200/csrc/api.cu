@@ -487,12 +487,14 @@ mtx_status mtx_compute_min_max_mip(mtx_context_t c, const mtx_volume *vol, const
     mip_layout(grid, L, out->levelExtent, out->levelOffset, &total);
     void *mm = nullptr;
     if ((r = dev_alloc(c, &mm, total * sizeof(uint2))) != MTX_OK) return r;
+    bool l1_done = false;
     prof_begin(prof, "MinMax_Leaf_Pass", c->stream);
-    r = launch_minmax_leaf(c, p, (uint2 *)mm, c->stream);
+    r = launch_minmax_leaf(c, p, (uint2 *)mm, c->stream, 0, L > 1 ? (uint2 *)mm + out->levelOffset[1] : nullptr,
+                           out->levelExtent[1], &l1_done);
     prof_end(prof, c->stream);
     if (r == MTX_OK && L > 1) {
         prof_begin(prof, "MinMax_Octree_Reduction", c->stream);
-        r = launch_pyramid(c, (uint2 *)mm, L, out->levelExtent, out->levelOffset, c->stream);
+        r = launch_pyramid(c, (uint2 *)mm, L, out->levelExtent, out->levelOffset, c->stream, l1_done ? 1 : 0);
         prof_end(prof, c->stream);
     }
     if (r != MTX_OK) {
@@ -741,13 +743,15 @@ mtx_status mtx_extract_plain_async(mtx_context_t c, const mtx_volume *vol, const
     }
     cudaStream_t s = c->stream;
     mtx_profiler *P = c->prof;
+    bool l1_done = false;
     prof_begin(P, "MinMax_Leaf_Pass", s);
-    r = launch_minmax_leaf(c, p, (uint2 *)c->leaf.ptr, s);
+    r = launch_minmax_leaf(c, p, (uint2 *)c->leaf.ptr, s, 0, L > 1 ? (uint2 *)c->leaf.ptr + off[1] : nullptr, ext[1],
+                           &l1_done);
     prof_end(P, s);
     if (r != MTX_OK) return r;
     if (L > 1) {
         prof_begin(P, "MinMax_Octree_Reduction", s);
-        r = launch_pyramid(c, (uint2 *)c->leaf.ptr, L, ext, off, s);
+        r = launch_pyramid(c, (uint2 *)c->leaf.ptr, L, ext, off, s, l1_done ? 1 : 0);
         prof_end(P, s);
         if (r != MTX_OK) return r;
     }

@@ -50,13 +50,19 @@ struct TmaLeafArgs {
     uint32_t X, Y, Z, GX, GY, GZ;
     uint32_t nXS, nYG, nZC, zchunk;
     uint32_t nitems;
+    uint32_t E1[3];  // extents of octree level 1 (written when the kernel's l1 is set)
 };
 
+// Octree level 1 in the same pass (l1 set; one block per lane, even z runs):
+// a texel is the min/max of 2 x 2 x 2 blocks -- two consecutive blocks of a
+// warp's z run, the x pair by shuffle, the y pair (warps w and w + 1) through
+// shared memory after the slice's barrier.  Blocks outside the grid count as
+// the identity {~0, 0}.
 template <typename T, int B>
 __global__ void __launch_bounds__(128) minmax_leaf_tma_kernel(const __grid_constant__ CUtensorMap map_main,
                                                                  const __grid_constant__ CUtensorMap map_halo,
                                                                  const TmaLeafArgs a, uint2 *__restrict__ leaf,
-                                                                 DevStatus *st) {
+                                                                 uint2 *__restrict__ l1, DevStatus *st) {
     using L16 = Lane16<T>;
     constexpr int V = L16::V;
     constexpr int SEG = 32 * V;
@@ -70,6 +76,7 @@ __global__ void __launch_bounds__(128) minmax_leaf_tma_kernel(const __grid_const
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t bars[S];
     __shared__ uint32_t s_fail;
+    __shared__ uint2 s_l1[4][32];  // level-1 y pairs: the z- and x-combined value of each warp's lanes
     const uint32_t tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
 
     if (tid == 0) {
@@ -136,6 +143,39 @@ __global__ void __launch_bounds__(128) minmax_leaf_tma_kernel(const __grid_const
 #pragma unroll
         for (int j = 0; j < NB; ++j) { amn[j] = ~0u; amx[j] = 0u; }
         uint32_t bz = bz0;
+        // level 1: the held even block of a z pair, and a texel waiting for its y pair
+        uint32_t zlo = ~0u, zhi = 0u, pz = 0;
+        bool pend = false;
+        const bool bx_in = row_on && x0 / B < a.GX;
+        auto l1_close = [&](uint32_t lo, uint32_t hi, uint32_t cbz) {
+            if constexpr (NB == 1) {
+                uint32_t vlo = bx_in ? lo : ~0u, vhi = bx_in ? hi : 0u;
+                if ((cbz & 1u) == 0) {
+                    zlo = vlo;
+                    zhi = vhi;
+                    if (cbz + 1 < a.GZ) return;  // the odd partner closes next
+                } else {
+                    vlo = min(vlo, zlo);
+                    vhi = max(vhi, zhi);
+                }
+                vlo = min(vlo, __shfl_xor_sync(0xffffffffu, vlo, LPB));
+                vhi = max(vhi, __shfl_xor_sync(0xffffffffu, vhi, LPB));
+                s_l1[w][lane] = make_uint2(vlo, vhi);
+                pz = cbz >> 1;
+                pend = true;
+            }
+        };
+        auto l1_finish = [&]() {  // after a barrier that follows l1_close
+            if constexpr (NB == 1) {
+                pend = false;
+                if ((w & 1u) == 0 && lane % (2 * LPB) == 0) {
+                    const uint2 m = s_l1[w][lane], o = s_l1[w + 1][lane];
+                    const uint32_t X1 = (x0 / B) >> 1, Y1 = by >> 1;
+                    if (X1 < a.E1[0] && Y1 < a.E1[1] && pz < a.E1[2])
+                        l1[((uint64_t)pz * a.E1[1] + Y1) * a.E1[0] + X1] = make_uint2(min(m.x, o.x), max(m.y, o.y));
+                }
+            }
+        };
         for (uint32_t z = zs; z <= ze; ++z, ++seq) {
             if (!mbar_wait_bounded(&bars[seq % S], (seq / S) & 1u)) {
                 if (lane == 0) {
@@ -205,6 +245,7 @@ __global__ void __launch_bounds__(128) minmax_leaf_tma_kernel(const __grid_const
             for (int j = 0; j < NB; ++j) { amn[j] = min(amn[j], smn[j]); amx[j] = max(amx[j], smx[j]); }
             if (z == bz * B + B) {
                 // halo slice of bz, first slice of bz + 1: write block bz
+                uint32_t clo = ~0u, chi = 0u;
 #pragma unroll
                 for (int j = 0; j < NB; ++j) {
                     uint32_t lo = amn[j], hi = amx[j];
@@ -217,7 +258,10 @@ __global__ void __launch_bounds__(128) minmax_leaf_tma_kernel(const __grid_const
                         leaf[((uint64_t)bz * a.GY + by) * a.GX + x0 / B + j] = make_uint2(lo, hi);
                     amn[j] = smn[j];
                     amx[j] = smx[j];
+                    clo = lo;
+                    chi = hi;
                 }
+                if (l1) l1_close(clo, chi, bz);
                 ++bz;
             }
             __syncthreads();  // every warp is done with this stage
@@ -227,8 +271,10 @@ __global__ void __launch_bounds__(128) minmax_leaf_tma_kernel(const __grid_const
                 break;
             }
             if (tid == 0) issue_next();
+            if (pend) l1_finish();
         }
         if (ok && bz < bz1) {
+            uint32_t clo = ~0u, chi = 0u;
 #pragma unroll
             for (int j = 0; j < NB; ++j) {
                 uint32_t lo = amn[j], hi = amx[j];
@@ -239,6 +285,13 @@ __global__ void __launch_bounds__(128) minmax_leaf_tma_kernel(const __grid_const
                 }
                 if (row_on && on && (lane % LPB) == 0)
                     leaf[((uint64_t)bz * a.GY + by) * a.GX + x0 / B + j] = make_uint2(lo, hi);
+                clo = lo;
+                chi = hi;
+            }
+            if (l1) {
+                l1_close(clo, chi, bz);
+                __syncthreads();
+                if (pend) l1_finish();
             }
         }
     }
@@ -372,7 +425,8 @@ static cudaError_t launch_generic(const Problem &p, uint2 *leaf, cudaStream_t s)
 }
 
 template <typename T, int B>
-static mtx_status launch_tma(mtx_context *c, const Problem &p, uint2 *leaf, cudaStream_t s, uint32_t zover) {
+static mtx_status launch_tma(mtx_context *c, const Problem &p, uint2 *leaf, cudaStream_t s, uint32_t zover,
+                             uint2 *l1, const uint32_t *l1ext, bool *l1_done) {
     constexpr uint32_t SEG = 32 * (16 / sizeof(T));
     CUtensorMap mmain, mhalo;
     mtx_status r = make_volume_tensor_map_box(c, p, SEG, kTmaRows(B), 1, &mmain);
@@ -392,6 +446,11 @@ static mtx_status launch_tma(mtx_context *c, const Problem &p, uint2 *leaf, cuda
     a.zchunk = zc;
     a.nZC = ceil_div(p.GZ, zc);
     a.nitems = a.nXS * a.nYG * a.nZC;
+    // level 1 in the same pass: one block per lane (16 / sizeof(T) <= B) and z runs of whole pairs
+    constexpr bool kOneBlockPerLane = 16 / sizeof(T) <= B;
+    const bool with_l1 = kOneBlockPerLane && l1 && l1ext && zc % 2 == 0;
+    for (int i = 0; i < 3; ++i) a.E1[i] = with_l1 ? l1ext[i] : 0u;
+    if (l1_done) *l1_done = with_l1;
     const uint32_t smem = kTmaStages(B) * kTmaStage(B);
     auto k = minmax_leaf_tma_kernel<T, B>;
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -401,7 +460,7 @@ static mtx_status launch_tma(mtx_context *c, const Problem &p, uint2 *leaf, cuda
     if (e != cudaSuccess) return cuda_fail(c, e, "minmax tma occupancy");
     occ = std::max(1, std::min(occ, kTmaCtasPerSm));
     const uint32_t grid = std::min<uint32_t>(a.nitems, (uint32_t)c->sm_count * (uint32_t)occ);
-    k<<<grid, 128, smem, s>>>(mmain, mhalo, a, leaf, &c->ctrl->status);
+    k<<<grid, 128, smem, s>>>(mmain, mhalo, a, leaf, with_l1 ? l1 : nullptr, &c->ctrl->status);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "minmax tma launch");
     return MTX_OK;
@@ -429,8 +488,10 @@ static cudaError_t dispatch_leaf(const Problem &p, uint2 *leaf, cudaStream_t s, 
     }
 }
 
-mtx_status launch_minmax_leaf(mtx_context *c, const Problem &p, uint2 *leaf, cudaStream_t s, uint32_t zover) {
+mtx_status launch_minmax_leaf(mtx_context *c, const Problem &p, uint2 *leaf, cudaStream_t s, uint32_t zover,
+                              uint2 *l1, const uint32_t *l1ext, bool *l1_done) {
     cudaError_t e;
+    if (l1_done) *l1_done = false;
     if (!zover) zover = c->tuning.minmaxZChunk;
     const uint32_t sl = c->tuning.minmaxSlices;
     // TMA ring (the default for 2- and 4-byte voxels whose rows are 16-byte
@@ -441,15 +502,15 @@ mtx_status launch_minmax_leaf(mtx_context *c, const Problem &p, uint2 *leaf, cud
     if (tma) {
         if (p.dtype == MTX_DTYPE_U16) {
             switch (p.B) {
-            case 4: return launch_tma<uint16_t, 4>(c, p, leaf, s, zover);
-            case 8: return launch_tma<uint16_t, 8>(c, p, leaf, s, zover);
-            default: return launch_tma<uint16_t, 16>(c, p, leaf, s, zover);
+            case 4: return launch_tma<uint16_t, 4>(c, p, leaf, s, zover, l1, l1ext, l1_done);
+            case 8: return launch_tma<uint16_t, 8>(c, p, leaf, s, zover, l1, l1ext, l1_done);
+            default: return launch_tma<uint16_t, 16>(c, p, leaf, s, zover, l1, l1ext, l1_done);
             }
         }
         switch (p.B) {
-        case 4: return launch_tma<float, 4>(c, p, leaf, s, zover);
-        case 8: return launch_tma<float, 8>(c, p, leaf, s, zover);
-        default: return launch_tma<float, 16>(c, p, leaf, s, zover);
+        case 4: return launch_tma<float, 4>(c, p, leaf, s, zover, l1, l1ext, l1_done);
+        case 8: return launch_tma<float, 8>(c, p, leaf, s, zover, l1, l1ext, l1_done);
+        default: return launch_tma<float, 16>(c, p, leaf, s, zover, l1, l1ext, l1_done);
         }
     }
     switch (p.dtype) {
@@ -462,17 +523,17 @@ mtx_status launch_minmax_leaf(mtx_context *c, const Problem &p, uint2 *leaf, cud
 }
 
 mtx_status launch_pyramid(mtx_context *c, uint2 *all, int levels, const uint32_t ext[][3],
-                          const uint64_t *offset, cudaStream_t s) {
-    if (levels < 2) return MTX_OK;
+                          const uint64_t *offset, cudaStream_t s, int start) {
+    if (levels - start < 2) return MTX_OK;
     if (levels > kPyrMaxLevels) return fail(c, MTX_ERR_UNSUPPORTED, "too many mip levels");
     PyrAll P;
     memset(&P, 0, sizeof(P));
-    P.levels = levels;
-    for (int k = 0; k < levels; ++k) {
-        P.base[k] = all + offset[k];
-        for (int a = 0; a < 3; ++a) P.ext[k][a] = ext[k][a];
+    P.levels = levels - start;
+    for (int k = 0; k < P.levels; ++k) {
+        P.base[k] = all + offset[start + k];
+        for (int a = 0; a < 3; ++a) P.ext[k][a] = ext[start + k][a];
     }
-    const uint32_t tx = ceil_div(ext[0][0], 8), ty = ceil_div(ext[0][1], 8), tz = ceil_div(ext[0][2], 8);
+    const uint32_t tx = ceil_div(P.ext[0][0], 8), ty = ceil_div(P.ext[0][1], 8), tz = ceil_div(P.ext[0][2], 8);
     pyramid_all_kernel<<<tx * ty * tz, 512, 0, s>>>(P, tx, ty, tx * ty * tz, &c->ctrl->pyr_done);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "pyramid launch");

@@ -109,11 +109,14 @@ struct Problem {
 };
 
 // Stage 1: leaf min/max (B+1 halo) into leaf[nblocks] (uint2 {min,max}).
+// Given l1 and its extents, the TMA pass may also write octree level 1 there;
+// *l1_done says whether it did.
 mtx_status launch_minmax_leaf(mtx_context *c, const Problem &p, uint2 *leaf, cudaStream_t s,
-                              uint32_t zchunk_override = 0);
-// Octree levels 1.. from level 0 (already in all_levels at offset 0).
+                              uint32_t zchunk_override = 0, uint2 *l1 = nullptr, const uint32_t *l1ext = nullptr,
+                              bool *l1_done = nullptr);
+// Octree levels start+1.. from level start (already in all_levels at offset[start]).
 mtx_status launch_pyramid(mtx_context *c, uint2 *all_levels, int levels, const uint32_t ext[][3],
-                          const uint64_t *offset, cudaStream_t s);
+                          const uint64_t *offset, cudaStream_t s, int start = 0);
 
 // Stage 2: ordered compaction of active blocks.
 //   ids[rank] = block id, rank_map[id] = rank (0xffffffff if inactive),

@@ -3,7 +3,9 @@ rows are 16-byte aligned) against the oracle's (B+1)^3 block min/max, bit for
 bit, and against the load-based pass (min/max slices 1, 2, 4) on the same
 volume.  Shapes cover partial x-strips (X not a multiple of the 512-byte
 strip), partial groups of four block rows, partial runs of z slabs, volumes
-smaller than one strip, and every block edge the pass takes."""
+smaller than one strip, and every block edge the pass takes.  With one block
+per lane and even z runs the pass also writes octree level 1; odd block-grid
+extents give level-1 texels with missing children in x, y and z."""
 import numpy as np
 import pytest
 
@@ -21,6 +23,9 @@ CASES = [
     ((40, 36, 132), np.float32, 8, 0),   # float: 128-voxel strips
     ((31, 29, 20), np.float32, 4, 0),
     ((48, 48, 136), np.float32, 16, 1),  # runs of one slab
+    ((72, 40, 264), np.uint16, 8, 2),    # level 1 in the pass: grid 33 x 5 x 9, the last slab unpaired
+    ((56, 24, 136), np.float32, 8, 4),   # level 1, two lanes a block: grid 17 x 3 x 7
+    ((40, 40, 264), np.uint16, 16, 2),   # level 1, block 16: grid 17 x 3 x 3
 ]
 
 
