@@ -4,12 +4,15 @@
 //
 // meshtrex scans within a workgroup and then takes one atomicAdd per
 // workgroup, so the compacted list is ordered only inside a workgroup.  Here
-// each CTA takes a tile of 1024 consecutive block ids by ticket, counts its
+// each CTA takes a tile of consecutive block ids by ticket (4096 a tile, 16
+// per thread, so that a 1024^3 volume at block 8 is one wave of CTAs; 1024 in
+// the no-allocation entry point, whose scratch is sized for them), counts its
 // active blocks (warp scan + CTA scan), and resolves its global offset with a
 // single-pass decoupled look-back over the tiles before it: the list comes out
 // in ascending block order, which is the order the CPU rule produces.  It
 // also writes the rank of every block (0xffffffff for inactive ones), which
 // the extraction uses to find a neighbouring block's vertices.
+#include <cstddef>
 #include <mutex>
 
 #include "mtx_internal.h"
@@ -17,12 +20,15 @@
 namespace mtx {
 
 constexpr int kFilterThreads = 256;
-constexpr int kFilterItems = 4;
+constexpr int kFilterItems = 16;       // blocks a thread: tiles of 4096
+constexpr int kNoallocItems = 4;       // tiles of 1024 in mtx_filter_active_blocks_noalloc
 constexpr int kFilterTile = kFilterThreads * kFilterItems;
+constexpr int kNoallocTile = kFilterThreads * kNoallocItems;
 
 // tile status word: [31:30] flag (0 empty, 1 aggregate, 2 inclusive, 3 aborted), [29:0] count
 constexpr uint32_t kFlagAgg = 1u, kFlagInc = 2u, kFlagAbort = 3u;
 
+template <int ITEMS>
 __global__ void __launch_bounds__(kFilterThreads)
     filter_compact_kernel(const uint2 *__restrict__ leaf, uint64_t nblocks, uint32_t ntiles, uint32_t dtype,
                           float iso, uint32_t *__restrict__ ids, uint32_t *__restrict__ rank_map,
@@ -38,18 +44,21 @@ __global__ void __launch_bounds__(kFilterThreads)
     const uint32_t t = s_tile;
     if (t >= ntiles) return;
 
-    const uint64_t base = (uint64_t)t * kFilterTile + (uint64_t)threadIdx.x * kFilterItems;
-    uint32_t f[kFilterItems];
-    if (base + kFilterItems <= nblocks) {
+    const uint64_t base = (uint64_t)t * (kFilterThreads * ITEMS) + (uint64_t)threadIdx.x * ITEMS;
+    uint32_t f[ITEMS];
+    if (base + ITEMS <= nblocks) {
         const uint4 *p = reinterpret_cast<const uint4 *>(leaf + base);
-        uint4 a = __ldg(p), b = __ldg(p + 1);
-        f[0] = block_active(dtype, a.x, a.y, iso);
-        f[1] = block_active(dtype, a.z, a.w, iso);
-        f[2] = block_active(dtype, b.x, b.y, iso);
-        f[3] = block_active(dtype, b.z, b.w, iso);
+        uint4 v[ITEMS / 2];
+#pragma unroll
+        for (int i = 0; i < ITEMS / 2; ++i) v[i] = __ldg(p + i);  // all loads before any use
+#pragma unroll
+        for (int i = 0; i < ITEMS / 2; ++i) {
+            f[2 * i] = block_active(dtype, v[i].x, v[i].y, iso);
+            f[2 * i + 1] = block_active(dtype, v[i].z, v[i].w, iso);
+        }
     } else {
 #pragma unroll
-        for (int i = 0; i < kFilterItems; ++i) {
+        for (int i = 0; i < ITEMS; ++i) {
             f[i] = 0;
             if (base + i < nblocks) {
                 uint2 v = leaf[base + i];
@@ -57,7 +66,9 @@ __global__ void __launch_bounds__(kFilterThreads)
             }
         }
     }
-    const uint32_t c = f[0] + f[1] + f[2] + f[3];
+    uint32_t c = 0;
+#pragma unroll
+    for (int i = 0; i < ITEMS; ++i) c += f[i];
     uint32_t total;
     const uint32_t excl = cta_exclusive_scan<kFilterThreads>(c, s_tmp, &total);
 
@@ -108,9 +119,9 @@ __global__ void __launch_bounds__(kFilterThreads)
     if (s_abort) return;
     uint32_t r = s_prefix + excl;
     // rank of every block of the tile: its rank if active, else kNoRank
-    uint32_t rk[kFilterItems];
+    uint32_t rk[ITEMS];
 #pragma unroll
-    for (int i = 0; i < kFilterItems; ++i) {
+    for (int i = 0; i < ITEMS; ++i) {
         rk[i] = 0xffffffffu;
         if (f[i]) {
             const uint32_t id = (uint32_t)(base + i);
@@ -120,11 +131,14 @@ __global__ void __launch_bounds__(kFilterThreads)
             ++r;
         }
     }
-    if (base + kFilterItems <= nblocks) {
-        *reinterpret_cast<uint4 *>(rank_map + base) = make_uint4(rk[0], rk[1], rk[2], rk[3]);
+    if (base + ITEMS <= nblocks) {
+#pragma unroll
+        for (int i = 0; i < ITEMS / 4; ++i)
+            reinterpret_cast<uint4 *>(rank_map + base)[i] = make_uint4(rk[4 * i], rk[4 * i + 1], rk[4 * i + 2],
+                                                                       rk[4 * i + 3]);
     } else {
 #pragma unroll
-        for (int i = 0; i < kFilterItems; ++i)
+        for (int i = 0; i < ITEMS; ++i)
             if (base + i < nblocks) rank_map[base + i] = rk[i];
     }
     if (t == ntiles - 1 && threadIdx.x == 0) *count_out = s_prefix + total;
@@ -137,9 +151,14 @@ mtx_status launch_filter(mtx_context *c, const Problem &p, const uint2 *leaf, ui
     mtx_status rs = scratch_reserve(c, c->filter_status, sizeof(uint32_t) * (size_t)ntiles);
     if (rs != MTX_OK) return rs;
     MTX_CUDA(c, cudaMemsetAsync(c->filter_status.ptr, 0, sizeof(uint32_t) * (size_t)ntiles, s));
-    MTX_CUDA(c, cudaMemsetAsync(&c->ctrl->filter_ticket, 0, sizeof(uint32_t), s));
-    MTX_CUDA(c, cudaMemsetAsync(count, 0, sizeof(uint32_t), s));
-    filter_compact_kernel<<<ntiles, kFilterThreads, 0, s>>>(
+    if (count == &c->ctrl->active_count) {  // ticket, count ticket (reset by the count pass too) and count: one memset
+        static_assert(offsetof(Ctrl, active_count) == offsetof(Ctrl, filter_ticket) + 8, "Ctrl layout");
+        MTX_CUDA(c, cudaMemsetAsync(&c->ctrl->filter_ticket, 0, 3 * sizeof(uint32_t), s));
+    } else {
+        MTX_CUDA(c, cudaMemsetAsync(&c->ctrl->filter_ticket, 0, sizeof(uint32_t), s));
+        MTX_CUDA(c, cudaMemsetAsync(count, 0, sizeof(uint32_t), s));
+    }
+    filter_compact_kernel<kFilterItems><<<ntiles, kFilterThreads, 0, s>>>(
         leaf, p.nblocks, ntiles, p.dtype, p.iso, ids, rank_map, count, count_status,
         (uint32_t *)c->filter_status.ptr, &c->ctrl->filter_ticket, &c->ctrl->status);
     cudaError_t e = cudaGetLastError();
@@ -198,8 +217,8 @@ extern "C" mtx_status mtx_filter_active_blocks_noalloc(const uint32_t *leaf_minm
     using namespace mtx;
     if (!leaf_minmax || !compacted_ids || !block_rank || !active_count || dtype > MTX_DTYPE_F32 || total_blocks == 0)
         return MTX_ERR_INVALID_ARG;
-    if (total_blocks > (uint64_t)kNoallocMaxTiles * kFilterTile) return MTX_ERR_CAPACITY;
-    const uint32_t ntiles = (uint32_t)((total_blocks + kFilterTile - 1) / kFilterTile);
+    if (total_blocks > (uint64_t)kNoallocMaxTiles * kNoallocTile) return MTX_ERR_CAPACITY;
+    const uint32_t ntiles = (uint32_t)((total_blocks + kNoallocTile - 1) / kNoallocTile);
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess) {
         cudaGetLastError();
@@ -223,9 +242,9 @@ extern "C" mtx_status mtx_filter_active_blocks_noalloc(const uint32_t *leaf_minm
         cudaGetLastError();
         return MTX_ERR_CUDA;
     }
-    filter_compact_kernel<<<ntiles, kFilterThreads, 0, s>>>(reinterpret_cast<const uint2 *>(leaf_minmax), total_blocks,
-                                                           ntiles, dtype, isovalue, compacted_ids, block_rank,
-                                                           active_count, nullptr, sc, sc + kNoallocTicket, st);
+    filter_compact_kernel<kNoallocItems><<<ntiles, kFilterThreads, 0, s>>>(
+        reinterpret_cast<const uint2 *>(leaf_minmax), total_blocks, ntiles, dtype, isovalue, compacted_ids, block_rank,
+        active_count, nullptr, sc, sc + kNoallocTicket, st);
     if (cudaGetLastError() != cudaSuccess) return MTX_ERR_CUDA;
     return MTX_OK;
 }
