@@ -892,12 +892,23 @@ __device__ __forceinline__ void count_block(const Problem &p, const WPlan &pl, u
         uint4 *dst = reinterpret_cast<uint4 *>(state);
         for (uint32_t i = lane; i < pl.state_bytes / 16; i += 32) dst[i] = src[i];
     }
-    for (uint32_t e = lane; e < 3 * BB; e += 32) {
-        const uint32_t f = fdiv(e, pl.rBB), i = e - f * BB, b = fdiv(i, pl.rB), a = i - b * B;
-        const uint32_t x = f == 0 ? 0 : a, y = f == 0 ? a : (f == 1 ? 0 : b), z = f == 2 ? 0 : b;
-        const uint32_t q = z * B + y;
-        fr[e] = voxel_prefix(cross, vp, BB, q, x) | (voxel_mask(cross, BB, q, x) << 24);
+    // y == 0 and z == 0 faces: lane l < 2B walks row (y = 0, z = l) or (y = l - B,
+    // z = 0) along x, the first vertex running up by each voxel's owned edges
+    if (lane < 2 * B) {
+        const bool yface = lane < B;
+        const uint32_t q = yface ? lane * B : lane - B;
+        uint32_t *o = fr + (yface ? BB + lane * B : 2 * BB + (lane - B) * B);
+        const uint32_t xc = cross[q], yc = cross[BB + q], zc = cross[2 * BB + q];
+        uint32_t run = vp[q];
+        for (uint32_t x = 0; x < B; ++x) {
+            const uint32_t m = ((xc >> x) & 1u) | (((yc >> x) & 1u) << 1) | (((zc >> x) & 1u) << 2);
+            o[x] = run | (m << 24);
+            run += __popc(m);
+        }
     }
+    // x == 0 face: record z*B + y is voxel (0, y, z), the first of row q = z*B + y
+    for (uint32_t q = lane; q < BB; q += 32)
+        fr[q] = vp[q] | (((cross[q] & 1u) | ((cross[BB + q] & 1u) << 1) | ((cross[2 * BB + q] & 1u) << 2)) << 24);
 }
 
 // Emit body of one block whose tile is staged and whose context layer has
