@@ -204,18 +204,11 @@ __device__ __forceinline__ void block_counts_balanced(const Problem &p, const WP
 __device__ __forceinline__ void count_block_balanced(const Problem &p, const WPlan &pl, unsigned char *ws,
                                                      const Geo &g, const uint8_t *ntab, mtx_meshlet_descriptor *dr,
                                                      uint32_t *fr) {
-    const uint32_t lane = threadIdx.x & 31, B = pl.B, BB = pl.BB;
-    const uint32_t *cross = reinterpret_cast<const uint32_t *>(ws + pl.off_cross);
-    const uint32_t *vp = reinterpret_cast<const uint32_t *>(ws + pl.off_vp);
+    const uint32_t lane = threadIdx.x & 31;
     uint32_t bnv, bnt;
     block_counts_balanced(p, pl, ws, g, ntab, true, bnv, bnt);
     if (lane == 0) *reinterpret_cast<uint2 *>(&dr->vertexCount) = make_uint2(bnv, bnt);
-    for (uint32_t e = lane; e < 3 * BB; e += 32) {
-        const uint32_t f = fdiv(e, pl.rBB), i = e - f * BB, b = fdiv(i, pl.rB), a = i - b * B;
-        const uint32_t x = f == 0 ? 0 : a, y = f == 0 ? a : (f == 1 ? 0 : b), z = f == 2 ? 0 : b;
-        const uint32_t q = z * B + y;
-        fr[e] = voxel_prefix(cross, vp, BB, q, x) | (voxel_mask(cross, BB, q, x) << 24);
-    }
+    write_face_records(pl, ws, fr);
 }
 
 // ---------------------------------------------------------- vertex table

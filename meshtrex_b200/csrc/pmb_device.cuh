@@ -872,26 +872,13 @@ __device__ __forceinline__ void gather_finish(const WPlan &pl, uint32_t nb_vb, c
     }
 }
 
-// Count body of one block whose tile is staged: the (vertices, triangles)
-// counts into *dr and the low-face records -- block-relative prefix | mask
-// << 24 of the voxels with x == 0 (index z*B+y), y == 0 (BB + z*B+x) and
-// z == 0 (2BB + y*B+x) -- into fr.
-template <typename T>
-__device__ __forceinline__ void count_block(const Problem &p, const WPlan &pl, unsigned char *ws, uint32_t buf,
-                                            const Geo &g, const uint8_t *ntab, uint8_t *cases_out,
-                                            mtx_meshlet_descriptor *dr, uint32_t *fr, uint8_t *state) {
+// The block's low-face records from its crossing rows and row prefixes:
+// block-relative first vertex | owned-edge mask << 24 of the voxels with
+// x == 0 (index z*B + y), y == 0 (BB + z*B + x) and z == 0 (2BB + y*B + x).
+__device__ __forceinline__ void write_face_records(const WPlan &pl, const unsigned char *ws, uint32_t *fr) {
     const uint32_t lane = threadIdx.x & 31, B = pl.B, BB = pl.BB;
     const uint32_t *cross = reinterpret_cast<const uint32_t *>(ws + pl.off_cross);
     const uint32_t *vp = reinterpret_cast<const uint32_t *>(ws + pl.off_vp);
-    build_rows<T>(p, pl, ws, buf, g);
-    uint32_t bnv, bnt;
-    block_counts(p, pl, ws, g, ntab, true, cases_out, bnv, bnt, state != nullptr);
-    if (lane == 0) *reinterpret_cast<uint2 *>(&dr->vertexCount) = make_uint2(bnv, bnt);
-    if (state) {  // the block state for the emit pass: 16-byte words, coalesced
-        const uint4 *src = reinterpret_cast<const uint4 *>(ws + pl.off_cross);
-        uint4 *dst = reinterpret_cast<uint4 *>(state);
-        for (uint32_t i = lane; i < pl.state_bytes / 16; i += 32) dst[i] = src[i];
-    }
     // y == 0 and z == 0 faces: lane l < 2B walks row (y = 0, z = l) or (y = l - B,
     // z = 0) along x, the first vertex running up by each voxel's owned edges
     if (lane < 2 * B) {
@@ -909,6 +896,27 @@ __device__ __forceinline__ void count_block(const Problem &p, const WPlan &pl, u
     // x == 0 face: record z*B + y is voxel (0, y, z), the first of row q = z*B + y
     for (uint32_t q = lane; q < BB; q += 32)
         fr[q] = vp[q] | (((cross[q] & 1u) | ((cross[BB + q] & 1u) << 1) | ((cross[2 * BB + q] & 1u) << 2)) << 24);
+}
+
+// Count body of one block whose tile is staged: the (vertices, triangles)
+// counts into *dr and the low-face records -- block-relative prefix | mask
+// << 24 of the voxels with x == 0 (index z*B+y), y == 0 (BB + z*B+x) and
+// z == 0 (2BB + y*B+x) -- into fr.
+template <typename T>
+__device__ __forceinline__ void count_block(const Problem &p, const WPlan &pl, unsigned char *ws, uint32_t buf,
+                                            const Geo &g, const uint8_t *ntab, uint8_t *cases_out,
+                                            mtx_meshlet_descriptor *dr, uint32_t *fr, uint8_t *state) {
+    const uint32_t lane = threadIdx.x & 31;
+    build_rows<T>(p, pl, ws, buf, g);
+    uint32_t bnv, bnt;
+    block_counts(p, pl, ws, g, ntab, true, cases_out, bnv, bnt, state != nullptr);
+    if (lane == 0) *reinterpret_cast<uint2 *>(&dr->vertexCount) = make_uint2(bnv, bnt);
+    if (state) {  // the block state for the emit pass: 16-byte words, coalesced
+        const uint4 *src = reinterpret_cast<const uint4 *>(ws + pl.off_cross);
+        uint4 *dst = reinterpret_cast<uint4 *>(state);
+        for (uint32_t i = lane; i < pl.state_bytes / 16; i += 32) dst[i] = src[i];
+    }
+    write_face_records(pl, ws, fr);
 }
 
 // Emit body of one block whose tile is staged and whose context layer has
