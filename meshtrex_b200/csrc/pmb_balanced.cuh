@@ -54,7 +54,8 @@ __host__ __device__ inline WPlan make_wplan_balanced(uint32_t B) {
     p.off_jobs = o;
     o = align_up(o + 4 * kRing, 16);
     p.off_vp = p.off_jobs;  // 4 * BB <= 4 * kRing for B <= 16
-    p.off_nvid = p.off_nm = p.off_tp = 0;  // unused
+    p.off_tp = p.off_tile[0];  // the count phase's triangle prefixes: the tile is dead there
+    p.off_nvid = p.off_nm = 0;  // unused
     p.bytes = o;
     return p;
 }
@@ -69,7 +70,12 @@ __host__ __device__ inline WPlan make_wplan_balanced(uint32_t B) {
 template <typename S>
 __device__ __forceinline__ void tile_load_rows_from(const Problem &p, const WPlan &pl, unsigned char *ws,
                                                     const Geo &g) {
-    constexpr uint32_t kLdgBatch = 8;
+    // four loads a lane in flight: the loop is inlined six times (three
+    // dtypes, count and emit phases) and a smaller kernel keeps the
+    // instruction cache from stalling the warps (batched mix: 35.7 ms at
+    // eight, 33.5 ms at four, 34.7 ms at two; one loop for all dtypes with a
+    // per-load branch, 34.6 ms)
+    constexpr uint32_t kLdgBatch = 4;
     const S *vol = reinterpret_cast<const S *>(p.vol);
     float *tile = reinterpret_cast<float *>(ws + pl.off_tile[0]);
     uint32_t *words = reinterpret_cast<uint32_t *>(ws + pl.off_list);
@@ -177,30 +183,20 @@ __device__ __forceinline__ uint32_t listed_case(const WPlan &pl, const uint32_t 
     return cell_case(rows, pl.B1, x, y, z);
 }
 
-// Crossing masks and vertex prefixes per row (block_counts without
-// triangles), then the triangle count over the listed mixed cells.
+// Crossing masks and vertex prefixes per row (block_counts), and with
+// want_tris the block's triangle count by the row walk of block_counts (the
+// count phase; its triangle prefixes land in the tile, dead by then).  The
+// walk takes fewer instructions and less code than listing the mixed cells
+// and counting them 32 at a time (batched mix 33.5 -> 32.6 ms).
 __device__ __forceinline__ void block_counts_balanced(const Problem &p, const WPlan &pl, unsigned char *ws,
                                                       const Geo &g, const uint8_t *ntab, bool want_tris,
                                                       uint32_t &nv, uint32_t &nt) {
-    const uint32_t lane = threadIdx.x & 31;
-    block_counts(p, pl, ws, g, ntab, false, nullptr, nv, nt);
-    nt = 0;
-    if (!want_tris) return;
-    const uint32_t *rows = reinterpret_cast<const uint32_t *>(ws + pl.off_rows);
-    const uint32_t nm = list_block<kMixedCells>(p, pl, g, ws);
-    const uint16_t *list = reinterpret_cast<const uint16_t *>(ws + pl.off_list);
-    for (uint32_t c0 = 0; c0 < nm; c0 += 32) {
-        uint32_t n = 0;
-        if (c0 + lane < nm) {
-            uint32_t ti;
-            n = ntab[listed_case(pl, rows, list[c0 + lane], ti)];
-        }
-        nt += __reduce_add_sync(0xffffffffu, n);
-    }
+    block_counts(p, pl, ws, g, ntab, want_tris, nullptr, nv, nt);
+    if (!want_tris) nt = 0;
 }
 
-// Count body (count_block) with the balanced triangle count, for a block
-// whose tile and inside masks tile_load_rows staged.
+// Count body (count_block) of the batched kernel, for a block whose tile and
+// inside masks tile_load_rows staged.
 __device__ __forceinline__ void count_block_balanced(const Problem &p, const WPlan &pl, unsigned char *ws,
                                                      const Geo &g, const uint8_t *ntab, mtx_meshlet_descriptor *dr,
                                                      uint32_t *fr) {
