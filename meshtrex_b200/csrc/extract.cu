@@ -3,15 +3,17 @@
 // marching_cubes_pmb.mesh.glsl:185-393, drawn by extractionManager.cpp:638-640).
 //
 // One warp owns one active block at a time; a CTA runs several such warps
-// that share only the case tables.  Each warp double-buffers the (B+1)^3
-// voxel tile of its block in shared memory (a TMA 3D tile, or plain loads
-// when the volume's rows are not 16-byte aligned), so the next block's tile
-// is in flight while the current one is processed.
+// that share only the case tables (and, in the emit pass, the context-layer
+// map).  Each warp stages the (B+1)^3 voxel tile of its block in shared
+// memory (a TMA 3D tile, or plain loads when the volume's rows are not
+// 16-byte aligned); the next block's tile is issued as soon as the current
+// block is done.
 //
-//  count pass  per-block vertex/triangle counts and low-face records
+//  count pass  per-block vertex/triangle counts, low-face records and, for
+//              B <= 8, the block state the emit pass takes over
 //  scan pass   decoupled look-back scan of the counts -> meshlet descriptors, totals
 //  emit pass   vertices (each exactly once) and triangles, indices resolved
-//              through the neighbours' face records
+//              through the block's voxel table and the neighbours' face records
 #include "pmb_device.cuh"
 
 namespace mtx {

@@ -35,10 +35,9 @@ __global__ void __launch_bounds__(128) minmax_leaf_vec_kernel(const T *__restric
 // the per-lane arithmetic of the load-based body: lane l owns 16 bytes of
 // every row, the +1 column of a block comes from the next lane by shuffle
 // (lane 31: from the halo box), and a slice at z = (bz+1)*B closes block bz
-// and opens bz+1; even and odd rows fold into separate registers so that the
-// dependent chains stay short.  Loads in flight live in shared memory (about
-// 35 KB per CTA), not in registers (40 per thread), so an SM keeps room for
-// the extraction kernels of other streams.
+// and opens bz+1; rows fold two at a time with three-input packed min/max.
+// Loads in flight live in shared memory (about 35 KB per CTA), not in
+// registers, so an SM keeps room for the extraction kernels of other streams.
 constexpr int kTmaRows(int B) { return 4 * B + 1; }
 constexpr uint32_t kTmaMain(int B) { return (uint32_t)kTmaRows(B) * 512u; }
 constexpr uint32_t kTmaHalo(int B) { return ((uint32_t)kTmaRows(B) * 16u + 127u) / 128u * 128u; }
@@ -311,15 +310,16 @@ __global__ void __launch_bounds__(128) minmax_leaf_generic_kernel(const T *__res
 }
 
 // Every octree level in one launch (minMaxOctreeReduce.comp.glsl:23-59 runs
-// one dispatch per level): a CTA of 512 threads loads an 8^3 tile of the leaf
-// level and writes the 4^3, 2^3 and 1 texels it covers in levels 1..3; the
-// CTA that finishes last builds levels 4.. from level 3 and zeroes the
-// counter (zero since the context's creation) for the next launch.  Each
-// texel is the min/max of its up-to-8 children; children past their level's
-// extent are skipped (minMaxOctreeReduce.comp.glsl:37-47), which the
-// identity {~0, 0} of the texels outside the leaf level's extent gives for
-// free.  The tile stays at 8^3 (4 KB of shared memory) so that the CTAs fit
-// beside the extraction kernels of other streams.
+// one dispatch per level): a CTA of 512 threads loads an 8^3 tile of the
+// launch's first level (the leaf level, or level 1 when the leaf pass wrote
+// it) and writes the 4^3, 2^3 and 1 texels it covers in the next three
+// levels; the CTA that finishes last builds the rest from the third and
+// zeroes the counter (zero since the context's creation) for the next
+// launch.  Each texel is the min/max of its up-to-8 children; children past
+// their level's extent are skipped (minMaxOctreeReduce.comp.glsl:37-47),
+// which the identity {~0, 0} of the texels outside the first level's extent
+// gives for free.  The tile stays at 8^3 (4 KB of shared memory) so that the
+// CTAs fit beside the extraction kernels of other streams.
 constexpr int kPyrMaxLevels = 32;
 struct PyrAll {
     uint2 *base[kPyrMaxLevels];

@@ -526,7 +526,7 @@ __device__ __forceinline__ float3 vertex_pos(const Problem &p, const WPlan &pl, 
 // Each lane walks the cut edges of its rows and writes one job per vertex
 // (voxel index | axis << 12) at the vertex's own position in a window of
 // kJobWin jobs; the warp then resolves the window 32 vertices at a time, one
-// per lane, staging positions in shared memory for coalesced stores.
+// per lane, each lane storing its own vertex record.
 // GENERIC selects the VertexData / NDC / normals options; the plain form
 // writes xyz in the voxel frame.  ANY: the tile holds the voxels converted to
 // T = float and the volume's own dtype is p.dtype (used for the normals).
