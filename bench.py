@@ -129,6 +129,25 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": n}
 
 
+def relaunch_ranks(gpus: int, argv) -> int | None:
+    """`--gpus N` (N > 1) run without torchrun around it: start N ranks of this
+    script under torchrun on this node (rendezvous on 127.0.0.1), with the same
+    arguments, and return their exit code.  None when there is nothing to do
+    (N = 1, or already a rank of a torchrun job)."""
+    if gpus <= 1 or os.environ.get("WORLD_SIZE"):
+        return None
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={gpus}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__)] + list(argv)
+    try:
+        return subprocess.run(cmd, timeout=3600).returncode
+    except subprocess.TimeoutExpired:
+        return 124
+
+
 def nproc():
     try:
         return len(os.sched_getaffinity(0))
@@ -137,6 +156,13 @@ def nproc():
 
 
 # --------------------------------------------------------------- CPU side
+def bench_config(ws):
+    """The workload description both arms print (the same keys and values)."""
+    return {"workload": workload(), "volume": [N, N, N], "block": BLOCK, "isovalues": list(ISOS),
+            "l2": "inputs larger than L2 (2 GiB volume streamed per extraction)",
+            "parallelism": f"replicas x{ws}" if ws > 1 else "single device"}
+
+
 def cpu_sample_volume(nz: int, device: str):
     """Middle z-slab of nz slices of the 1024^3 workload, as a host array."""
     from meshtrex_b200 import synth
@@ -146,29 +172,77 @@ def cpu_sample_volume(nz: int, device: str):
 
 
 def time_cpu_oracle(vol: np.ndarray, threads: int):
-    """One step of the CPU restatement on `vol`: the three isovalues."""
+    """One step of meshtrex's CPU path as the oracle restates it, on `vol`:
+    for each of the three isovalues, min/max over the (B+1)^3 blocks
+    (testMinMax.h:28-135), ordered compaction (blockFilteringTestUtils.h:438-478)
+    and PMB marching cubes with the vertex and index buffers written
+    (extractionTestUtils.cpp:34-36 for the vertex placement).  Returns
+    (seconds, triangles, meshes)."""
     from oracle import oracle as O
     t0 = time.perf_counter()
-    tris = 0
+    tris, meshes = 0, []
     for iso in ISOS:
-        _, _, t = O.pipeline(vol, BLOCK, iso, nthreads=threads)
-        tris += t
-    return time.perf_counter() - t0, tris
+        m = O.extract(vol, BLOCK, iso, nthreads=threads)
+        tris += m.n_triangles
+        meshes.append(m)
+    return time.perf_counter() - t0, tris, meshes
 
 
-def cpu_baseline(vol: np.ndarray, threads: int, target_s: float = 10.0):
-    """The oracle timed on the host cores on the same volume, repeated to ~target_s."""
+def cpu_run(vol: np.ndarray, threads: int, target_s: float, what: str):
+    """The oracle timed on `threads` host cores on `vol`, repeated to ~target_s."""
     secs, tris, reps = 0.0, 0, 0
     while reps == 0 or (secs < target_s and reps < 20):
-        s, t = time_cpu_oracle(vol, threads)
+        s, t, _ = time_cpu_oracle(vol, threads)
         secs += s
         tris += t
         reps += 1
     vox = 3 * vol.size * reps
     return {"value": vox / secs / 1e9, "unit": "Gvoxels/s", "cores": threads, "kind": "port",
-            "sample": (f"the whole {vol.shape[2]}x{vol.shape[1]}x{vol.shape[0]} uint16 volume at the three "
-                       f"isovalues, {reps} repetition(s), {secs:.2f} s"),
+            "sample": (f"{what}: {vol.shape[2]}x{vol.shape[1]}x{vol.shape[0]} uint16 at the three isovalues, "
+                       f"min/max + compaction + marching cubes with vertices and indices written, "
+                       f"{reps} repetition(s), {secs:.2f} s"),
             "tris_per_s": tris / secs}
+
+
+def cpu_baselines(host: np.ndarray, dev: str):
+    """All host threads on the whole volume, and one thread (meshtrex's CPU path
+    is single-threaded) on a middle z-slab sized for about 10 s."""
+    threads = nproc()
+    allcore = cpu_run(host, threads, 10.0, "whole volume")
+    probe, _ = cpu_sample_volume(32, dev)
+    s1, _, _ = time_cpu_oracle(probe, 1)
+    nz = int(max(16, min(N, 32 * 10.0 / max(s1, 1e-3))) // 8 * 8)
+    slab, z0 = cpu_sample_volume(nz, dev)
+    one = cpu_run(slab, 1, 10.0, f"middle z-slab z={z0}..{z0 + nz}")
+    return allcore, one
+
+
+def oracle_parity(host: np.ndarray, exts, threads: int):
+    """The oracle's full mesh of every isovalue of the step, on the same host
+    bytes as the GPU's volume, against the GPU's outputs bit for bit: active
+    blocks, vertex and triangle counts, vertex bits and index buffers."""
+    import hashlib
+    from oracle import oracle as O
+    per_iso = []
+    ok = True
+    for iso, e in zip(ISOS, exts):
+        c = e.counters.cpu().numpy().view(np.uint32)
+        V, T = int(c[0]), int(c[1]) // 3
+        ref = O.extract(host, BLOCK, iso, nthreads=threads)
+        gv = e.vertices[:V].cpu().numpy()
+        gi = e.indices[:T].cpu().numpy().view(np.uint32)
+        same = (int(c[4]) == 0 and int(c[3]) == len(ref.ids) and V == ref.n_vertices and T == ref.n_triangles
+                and np.array_equal(gv.view(np.uint32), ref.xyz.view(np.uint32))
+                and np.array_equal(gi, ref.indices))
+        ok = ok and same
+        h = hashlib.sha256()
+        h.update(gv.tobytes())
+        h.update(gi.tobytes())
+        per_iso.append({"isovalue": iso, "active_blocks": int(c[3]), "vertices": V, "triangles": T,
+                        "mesh_sha256": h.hexdigest()[:16], "match": bool(same)})
+    return {"oracle_match": bool(ok), "per_isovalue": per_iso,
+            "what": "oracle (CPU restatement, all host threads) on the same host bytes; active-block count, V, T, "
+                    "vertex float bits and index buffer compared exactly"}
 
 
 def run_reference(args):
@@ -177,9 +251,9 @@ def run_reference(args):
         return 0
     dev = "cuda" if torch.cuda.is_available() else "cpu"
     threads = nproc()
-    # calibrate the sample so that one step is ~10 s of CPU work
+    # calibrate the sample so that one step is ~10 s of CPU work and the run ~150 s
     probe, _ = cpu_sample_volume(min(N, 64), dev)
-    secs, _ = time_cpu_oracle(probe, threads)
+    secs, _, _ = time_cpu_oracle(probe, threads)
     pz = probe.shape[0]
     total_steps = args.steps + args.warmup
     budget = 150.0  # seconds for the whole run
@@ -190,7 +264,7 @@ def run_reference(args):
         time_cpu_oracle(vol, threads)
     t_all, tris_all = 0.0, 0
     for _ in range(args.steps):
-        s, t = time_cpu_oracle(vol, threads)
+        s, t, _ = time_cpu_oracle(vol, threads)
         t_all += s
         tris_all += t
     vox = 3 * vol.size * args.steps
@@ -199,11 +273,11 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * t_all / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u16",
             "data": "synthetic (seeded fBm ball, same generator as the GPU arm)",
-            "config": {"workload": workload(), "sample": f"1024x1024x{nz} middle z-slab per step",
-                       "block": BLOCK, "isovalues": list(ISOS), "parallelism": "CPU, all host threads"},
+            "config": bench_config(ws),
             "tris_per_s": tris_all / t_all,
             "cpu_baseline": {"value": value, "unit": "Gvoxels/s", "cores": threads, "kind": "port",
-                             "sample": f"1024x1024x{nz} middle z-slab (z={z0}..{z0 + nz}), 3 isovalues"},
+                             "sample": (f"1024x1024x{nz} middle z-slab (z={z0}..{z0 + nz}) per step, 3 isovalues, "
+                                        "min/max + compaction + marching cubes with vertices and indices written")},
             "e2e": {"value": value, "unit": "Gvoxels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -360,10 +434,8 @@ def run_mtx(args):
             "warmup": args.warmup, "ms_per_step": 1000.0 * t_max / steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u16",
             "data": "synthetic (seeded fBm ball generated on the device; no dataset)",
-            "config": {"workload": workload(), "volume": [N, N, N], "block": BLOCK, "isovalues": list(ISOS),
-                       "l2": "inputs larger than L2 (2 GiB volume streamed per extraction)",
-                       "streams": "the step's 3 extractions on 3 streams (one context each)",
-                       "parallelism": f"replicas x{ws}" if ws > 1 else "single GPU"},
+            "config": bench_config(ws),
+            "streams": "the step's 3 extractions on 3 streams (one context each)",
             "tris_per_s": tris_s, "vertices_per_step": sum(V), "triangles_per_step": sum(T),
             "stages_ms_per_extraction": per_stage,
             "roofline": {"bound": "hbm", "kernel": "minmax_leaf_tma_kernel<uint16_t,8>",
@@ -376,9 +448,13 @@ def run_mtx(args):
             "gpu_launches": launches_per_extraction(grid) * 3 * steps,
             "clocks": clk}
 
-    if rank == 0 and ws == 1 and not args.no_cpu:
+    if rank == 0 and not args.no_cpu:
         host = vol.cpu().view(torch.int16).numpy().view(np.uint16)
-        line["cpu_baseline"] = cpu_baseline(host, nproc())
+        line["parity"] = oracle_parity(host, exts, nproc())
+        if ws == 1:
+            allcore, one = cpu_baselines(host, "cuda")
+            line["cpu_baseline"] = allcore
+            line["cpu_baseline_1thread"] = one
         del host
 
     if not args.no_e2e:
@@ -766,7 +842,7 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="mtx", choices=["mtx", "reference"])
-    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline and oracle parity legs")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched 64-volume leg")
     ap.add_argument("--no-backward", action="store_true", help="skip the backward (adjoint) leg")
@@ -776,6 +852,9 @@ def main():
     ap.add_argument("--size", type=int, default=1024, help="volume edge (profiling runs only)")
     ap.add_argument("--cache", default="", help="raw file to read/write the generated volume")
     args = ap.parse_args()
+    rc = relaunch_ranks(args.gpus, sys.argv[1:])
+    if rc is not None:
+        return rc
     global N
     N = args.size
     if args.warmup < 3:

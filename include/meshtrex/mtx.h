@@ -21,6 +21,10 @@
  *    calls never do and can be captured in a CUDA graph.
  *  - Volumes are x fastest, then y, then z: voxel (x,y,z) is element
  *    z*X*Y + y*X + x (src/volume.h:8-12, src/testMinMax.h:97-101).
+ *  - The *_free calls release device memory in the order of the context's
+ *    stream, as cudaFreeAsync does, and do not wait: work queued on other
+ *    streams that still reads an output must finish (or be ordered before
+ *    the context's stream) before the output is freed.
  */
 #ifndef MESHTREX_MTX_H
 #define MESHTREX_MTX_H
@@ -240,6 +244,21 @@ float mtx_key_to_float(uint32_t dtype, uint32_t key);
 mtx_status mtx_compute_min_max_mip(mtx_context_t ctx, const mtx_volume *vol,
                                    const mtx_push_constants *pc, mtx_profiler_t prof,
                                    mtx_minmax_output *out);
+/* loadVolume's staging upload and computeMinMaxMip in one call, overlapped
+ * (src/volume.h:14-43, src/minMaxManager.cpp:63-225; meshtrex copies the
+ * whole volume, then dispatches, minMaxManager.cpp:115-133).  The host voxels
+ * go to a new device volume in z-slabs on a copy stream of the context; the
+ * leaf min/max of each slab of block layers runs on the context's stream as
+ * soon as its voxels and the one-voxel halo above them are on the device, so
+ * when the last slab lands only its own leaf pass and the octree remain.  The
+ * outputs equal mtx_volume_upload followed by mtx_compute_min_max_mip.  Does
+ * not wait: `host` must stay unchanged until the context's stream has done
+ * this work.  Pinned host memory (cudaHostAlloc, cudaHostRegister) is needed
+ * for the copies to overlap anything.  vol_out is owned by the caller (free it
+ * with mtx_volume_free), out as from mtx_compute_min_max_mip. */
+mtx_status mtx_upload_compute_min_max_mip(mtx_context_t ctx, const void *host, const uint32_t dims[3],
+                                          uint32_t dtype, const mtx_push_constants *pc, mtx_profiler_t prof,
+                                          mtx_volume *vol_out, mtx_minmax_output *out);
 mtx_status mtx_minmax_free(mtx_context_t ctx, mtx_minmax_output *mm);
 
 /* ------------------------------------------------------------ stage 2 */
@@ -264,15 +283,18 @@ mtx_status mtx_filtering_free(mtx_context_t ctx, mtx_filtering_output *filt);
  * stream, with its scratch in a fixed 256 KiB array inside the library
  * (every GPU that loads the library keeps it until the process exits), and
  * calls no allocator.
- *   leaf_minmax   device, {min,max} keys of total_blocks blocks (mip level 0)
+ *   leaf_minmax   device, 16-byte aligned: {min,max} keys of total_blocks blocks (mip level 0)
  *   compacted_ids device, total_blocks words: the active block ids, ascending
- *   block_rank    device, total_blocks words: rank of each block, 0xffffffff if inactive
+ *   block_rank    device, 16-byte aligned, total_blocks words: rank of each block, 0xffffffff if inactive
  *   active_count  device, one word
- *   device_status device, 4 words (optional): {mtx_status, site, info, info}
- *                 of an error a kernel met, zero otherwise
+ *   device_status device, 4 words (required): {mtx_status, site, info, info} of an
+ *                 error a kernel met (a look-back wait that gave up), zero otherwise;
+ *                 read it after the stream is done, before trusting the outputs
+ * A missing or misaligned pointer is MTX_ERR_INVALID_ARG before any work.
  * Limit: total_blocks <= 67,108,864 (65,536 tiles of 1024 blocks), else
- * MTX_ERR_CAPACITY before any work.  The first call on a device looks up the
- * array's device address; make that first call before any stream capture.
+ * MTX_ERR_CAPACITY before any work.  The first call in a CUDA context looks
+ * up the array's device address in that context (again after
+ * cudaDeviceReset); make that first call before any stream capture.
  * Every call reuses the same array, so calls that overlap on the GPU race:
  * issue them one after the other. */
 mtx_status mtx_filter_active_blocks_noalloc(const uint32_t *leaf_minmax, uint64_t total_blocks, uint32_t dtype,

@@ -161,6 +161,8 @@ SIGNATURES = [
     ("mtx_key_to_float", C.c_float, [C.c_uint32, C.c_uint32]),
     ("mtx_compute_min_max_mip", _ST, [_P, C.POINTER(Volume), C.POINTER(PushConstants), _P,
                                       C.POINTER(MinMaxOutput)]),
+    ("mtx_upload_compute_min_max_mip", _ST, [_P, _P, C.POINTER(C.c_uint32), C.c_uint32, C.POINTER(PushConstants),
+                                             _P, C.POINTER(Volume), C.POINTER(MinMaxOutput)]),
     ("mtx_minmax_free", _ST, [_P, C.POINTER(MinMaxOutput)]),
     ("mtx_filter_active_blocks", _ST, [_P, C.POINTER(MinMaxOutput), C.POINTER(PushConstants), _P,
                                        C.POINTER(FilteringOutput)]),

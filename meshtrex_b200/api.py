@@ -260,6 +260,23 @@ def compute_min_max_mip(ctx: Context, volume: L.Volume, pc: L.PushConstants, pro
     return MinMax(ctx, out)
 
 
+def upload_compute_min_max_mip(ctx: Context, host: np.ndarray, pc: L.PushConstants, profiler=None):
+    """mtx_upload_compute_min_max_mip: a host array [z, y, x] (pinned for the
+    copies to overlap) uploaded in z-slabs with the leaf min/max of each slab
+    running as it lands.  Returns (device volume, MinMax); the volume is owned:
+    release it with free_volume.  `host` must stay alive and unchanged until the
+    context's stream has done the work."""
+    a = host
+    assert a.flags.c_contiguous and a.ndim == 3
+    v = L.Volume()
+    out = L.MinMaxOutput()
+    d = (C.c_uint32 * 3)(a.shape[2], a.shape[1], a.shape[0])
+    L.check(L.lib().mtx_upload_compute_min_max_mip(ctx.handle, C.c_void_p(a.ctypes.data), d, _NP[a.dtype],
+                                                   C.byref(pc), _prof(profiler), C.byref(v), C.byref(out)),
+            "mtx_upload_compute_min_max_mip", ctx.handle)
+    return v, MinMax(ctx, out)
+
+
 def filter_active_blocks(ctx: Context, mm: MinMax, pc: L.PushConstants, profiler=None) -> Filtering:
     out = L.FilteringOutput()
     L.check(L.lib().mtx_filter_active_blocks(ctx.handle, C.byref(mm.out), C.byref(pc),

@@ -52,12 +52,17 @@ mtx_status cuda_fail(mtx_context *c, cudaError_t e, const char *what) {
 // Freed device buffers are kept for reuse.  The drop-in stages allocate their
 // outputs per call, as meshtrex's managers do, and cudaMalloc / cudaFree of
 // the same sizes call after call cost host time: milliseconds for a 2 GiB
-// volume, many more on a busy host.  A freed buffer first waits for its
-// device to go idle -- the guarantee cudaFree gives, that no stream still
-// uses it -- and then goes to a per-device list by exact size, from which an
-// allocation of that size takes it back.  At most kCacheBytes and
-// kCacheBuffers are kept per device; a failed cudaMalloc hands the device's
-// cached buffers back to the driver and tries again, and so does the
+// volume, many more on a busy host.  Freeing is ordered on the freeing
+// context's stream, as cudaFreeAsync is: the free records an event there and
+// the buffer goes to a per-device list by exact size; an allocation of that
+// size takes it back, and the taking context's stream waits for the event
+// (no host wait) if the old work is still running.  So a free never stalls
+// the device or the host, and work a caller queued on another stream that
+// still reads the buffer must be finished, or ordered before the freeing
+// context's stream, before the free call -- the contract of any
+// stream-ordered allocator.  At most kCacheBytes and kCacheBuffers are kept
+// per device; a failed cudaMalloc hands the device's cached buffers back to
+// the driver (after their events) and tries again, and so does the
 // destruction of a context (dev_cache_release).
 namespace {
 constexpr size_t kCacheBytes = 16ull << 30;
@@ -67,34 +72,38 @@ struct LiveAlloc {
     int device;
     size_t bytes;
 };
+struct IdleBuf {
+    void *ptr;
+    cudaEvent_t freed;  // recorded on the freeing stream; null when the free waited already
+};
 std::mutex g_alloc_mu;
-std::unordered_map<void *, LiveAlloc> g_live;                // every buffer dev_alloc handed out
-std::map<std::pair<int, size_t>, std::vector<void *>> g_idle;  // (device, bytes) -> freed buffers
+std::unordered_map<void *, LiveAlloc> g_live;                  // every buffer dev_alloc handed out
+std::map<std::pair<int, size_t>, std::vector<IdleBuf>> g_idle;  // (device, bytes) -> freed buffers
 size_t g_idle_bytes[kCacheDevices];
 uint32_t g_idle_count[kCacheDevices];
 
-void *take_idle(int device, size_t bytes) {
+bool take_idle(int device, size_t bytes, IdleBuf *out) {
     std::lock_guard<std::mutex> lk(g_alloc_mu);
     auto it = g_idle.find({device, bytes});
-    if (it == g_idle.end() || it->second.empty()) return nullptr;
-    void *p = it->second.back();
+    if (it == g_idle.end() || it->second.empty()) return false;
+    *out = it->second.back();
     it->second.pop_back();
     g_idle_bytes[device] -= bytes;
     --g_idle_count[device];
-    return p;
+    return true;
 }
 }  // namespace
 
 // Hands the freed buffers of `device` back to the driver (that device current).
 void dev_cache_release(int device) {
-    std::vector<void *> drop;
+    std::vector<IdleBuf> drop;
     {
         std::lock_guard<std::mutex> lk(g_alloc_mu);
         for (auto it = g_idle.begin(); it != g_idle.end();) {
             if (it->first.first == device) {
-                for (void *p : it->second) {
-                    drop.push_back(p);
-                    g_live.erase(p);
+                for (const IdleBuf &b : it->second) {
+                    drop.push_back(b);
+                    g_live.erase(b.ptr);
                 }
                 it = g_idle.erase(it);
             } else {
@@ -106,7 +115,13 @@ void dev_cache_release(int device) {
             g_idle_count[device] = 0;
         }
     }
-    for (void *p : drop) cudaFree(p);
+    for (const IdleBuf &b : drop) {
+        if (b.freed) {
+            cudaEventSynchronize(b.freed);
+            cudaEventDestroy(b.freed);
+        }
+        cudaFree(b.ptr);
+    }
 }
 
 mtx_status dev_alloc(mtx_context *c, void **p, size_t bytes) {
@@ -116,7 +131,21 @@ mtx_status dev_alloc(mtx_context *c, void **p, size_t bytes) {
     }
     if (bytes == 0) bytes = 16;
     const bool cached = c->device >= 0 && c->device < kCacheDevices;
-    if (cached && (*p = take_idle(c->device, bytes))) return MTX_OK;
+    IdleBuf idle{nullptr, nullptr};
+    if (cached && take_idle(c->device, bytes, &idle)) {
+        if (idle.freed) {
+            // the freeing stream's work must be done before this stream uses the buffer
+            cudaError_t e = cudaEventQuery(idle.freed);
+            if (e == cudaErrorNotReady) e = cudaStreamWaitEvent(c->stream, idle.freed, 0);
+            cudaEventDestroy(idle.freed);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                cudaEventSynchronize(idle.freed);
+            }
+        }
+        *p = idle.ptr;
+        return MTX_OK;
+    }
     cudaError_t e = cudaMalloc(p, bytes);
     if (e != cudaSuccess && cached) {
         cudaGetLastError();
@@ -135,7 +164,7 @@ mtx_status dev_alloc(mtx_context *c, void **p, size_t bytes) {
     return MTX_OK;
 }
 
-void dev_free(void *p) {
+void dev_free(mtx_context *c, void *p) {
     if (!p) return;
     LiveAlloc a{-1, 0};
     {
@@ -150,12 +179,24 @@ void dev_free(void *p) {
     int cur = -1;
     cudaGetDevice(&cur);
     if (cur != a.device) cudaSetDevice(a.device);
-    cudaDeviceSynchronize();  // as cudaFree: no stream may still use the buffer
+    // ordered on the freeing context's stream; without one, as cudaFree (the whole device)
+    cudaEvent_t ev = nullptr;
+    if (c && c->device == a.device) {
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventRecord(ev, c->stream) != cudaSuccess) {
+            cudaGetLastError();
+            if (ev) cudaEventDestroy(ev);
+            ev = nullptr;
+            cudaDeviceSynchronize();
+        }
+    } else {
+        cudaDeviceSynchronize();
+    }
     bool keep = false;
     {
         std::lock_guard<std::mutex> lk(g_alloc_mu);
         if (g_idle_bytes[a.device] + a.bytes <= kCacheBytes && g_idle_count[a.device] < kCacheBuffers) {
-            g_idle[{a.device, a.bytes}].push_back(p);
+            g_idle[{a.device, a.bytes}].push_back(IdleBuf{p, ev});
             g_idle_bytes[a.device] += a.bytes;
             ++g_idle_count[a.device];
             keep = true;
@@ -163,16 +204,21 @@ void dev_free(void *p) {
             g_live.erase(p);
         }
     }
-    if (!keep) cudaFree(p);
+    if (!keep) {
+        if (ev) {
+            cudaEventSynchronize(ev);
+            cudaEventDestroy(ev);
+        }
+        cudaFree(p);
+    }
     if (cur >= 0 && cur != a.device) cudaSetDevice(cur);
 }
 
 mtx_status scratch_reserve(mtx_context *c, Scratch &s, size_t bytes) {
     if (s.size >= bytes && s.ptr) return MTX_OK;
-    // grow geometrically; the stream must not still use the old block
+    // grow geometrically; the old block is released in the order of the stream
     if (s.ptr) {
-        cudaStreamSynchronize(c->stream);
-        dev_free(s.ptr);
+        dev_free(c, s.ptr);
         s.ptr = nullptr;
         s.size = 0;
     }
@@ -378,8 +424,9 @@ mtx_status mtx_context_destroy(mtx_context_t c) {
     cudaStreamSynchronize(c->stream);
     for (Scratch *s : {&c->filter_status, &c->count_status, &c->faces, &c->state, &c->leaf, &c->ids, &c->rank,
                        &c->desc, &c->misc, &c->adj_partial, &c->adj_iso})
-        dev_free(s->ptr);
+        dev_free(c, s->ptr);
     dev_cache_release(c->device);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     cudaFree(c->ctrl);
     cudaFreeHost(c->pinned);
     delete c;
@@ -419,7 +466,7 @@ mtx_status mtx_volume_upload(mtx_context_t c, const void *host, const uint32_t d
     if (r != MTX_OK) return r;
     cudaError_t e = cudaMemcpyAsync(d, host, bytes, cudaMemcpyHostToDevice, c->stream);
     if (e != cudaSuccess) {
-        dev_free(d);
+        dev_free(c, d);
         return cuda_fail(c, e, "volume upload");
     }
     memset(out, 0, sizeof(*out));
@@ -446,10 +493,7 @@ mtx_status mtx_volume_wrap(void *device_ptr, const uint32_t dims[3], uint32_t dt
 mtx_status mtx_volume_free(mtx_context_t c, mtx_volume *v) {
     if (!c || !v) return MTX_ERR_INVALID_ARG;
     DeviceGuard g(c->device);
-    if (v->owned && v->data.ptr) {
-        cudaStreamSynchronize(c->stream);
-        dev_free(v->data.ptr);
-    }
+    if (v->owned && v->data.ptr) dev_free(c, v->data.ptr);
     memset(v, 0, sizeof(*v));
     return MTX_OK;
 }
@@ -498,7 +542,7 @@ mtx_status mtx_compute_min_max_mip(mtx_context_t c, const mtx_volume *vol, const
         prof_end(prof, c->stream);
     }
     if (r != MTX_OK) {
-        dev_free(mm);
+        dev_free(c, mm);
         memset(out, 0, sizeof(*out));
         return r;
     }
@@ -514,11 +558,117 @@ mtx_status mtx_compute_min_max_mip(mtx_context_t c, const mtx_volume *vol, const
     return MTX_OK;
 }
 
+// Upload and leaf min/max overlapped (no meshtrex counterpart as one call:
+// meshtrex stages the whole volume, then dispatches, minMaxManager.cpp:115-133).
+// The volume goes to the device in slabs of S block layers on the context's
+// copy stream; the leaf pass of slab k runs on the context's stream once
+// slab k + 1 has landed (its first voxel slice is slab k's +z halo), as a
+// sub-problem over block layers [k*S, (k+1)*S) of the same grid.  The octree
+// follows the last slab.
+mtx_status mtx_upload_compute_min_max_mip(mtx_context_t c, const void *host, const uint32_t dims[3], uint32_t dtype,
+                                          const mtx_push_constants *pc, mtx_profiler_t prof, mtx_volume *vol_out,
+                                          mtx_minmax_output *out) {
+    if (!c || !host || !dims || !pc || !vol_out || !out)
+        return c ? fail(c, MTX_ERR_INVALID_ARG, "null argument") : MTX_ERR_INVALID_ARG;
+    if (dtype > MTX_DTYPE_F32 || !dims[0] || !dims[1] || !dims[2]) return fail(c, MTX_ERR_INVALID_ARG, "bad volume");
+    if (!prof) prof = c->prof;
+    DeviceGuard g(c->device);
+    memset(vol_out, 0, sizeof(*vol_out));
+    memset(out, 0, sizeof(*out));
+    mtx_volume v{};
+    for (int a = 0; a < 3; ++a) v.dims[a] = dims[a];
+    v.dtype = dtype;
+    v.owned = 1;
+    const uint64_t bytes = nvox(dims) * dtype_size(dtype);
+    v.data.size = bytes;
+    v.data.ptr = reinterpret_cast<void *>(uintptr_t(16));  // placeholder for the checks below
+    mtx_status r = check_pc(c, &v, pc);
+    if (r != MTX_OK) return r;
+    if (!c->copy_stream) MTX_CUDA(c, cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    const Problem p0 = make_problem(&v, pc->blockDim[0], pc->isovalue);
+    const uint32_t grid[3] = {p0.GX, p0.GY, p0.GZ};
+    const int L = mip_levels(grid);
+    if (L > MTX_MAX_MIP_LEVELS) return fail(c, MTX_ERR_UNSUPPORTED, "too many mip levels");
+    uint64_t total = 0;
+    mip_layout(grid, L, out->levelExtent, out->levelOffset, &total);
+    void *dv = nullptr, *mm = nullptr;
+    if ((r = dev_alloc(c, &dv, bytes)) != MTX_OK) return r;
+    if ((r = dev_alloc(c, &mm, total * sizeof(uint2))) != MTX_OK) {
+        dev_free(c, dv);
+        return r;
+    }
+    v.data.ptr = dv;
+    // slabs of S block layers: about 16 of them, each copy tens of MB or more
+    const uint32_t B = p0.B, S = std::max<uint32_t>(1, ceil_div(p0.GZ, 16));
+    const uint32_t nslab = ceil_div(p0.GZ, S);
+    const uint64_t slice = (uint64_t)dims[0] * dims[1] * dtype_size(dtype);
+    std::vector<cudaEvent_t> landed(nslab, nullptr);
+    cudaEvent_t ready = nullptr;
+    auto cleanup = [&]() {
+        for (cudaEvent_t e : landed)
+            if (e) cudaEventDestroy(e);
+        if (ready) cudaEventDestroy(ready);
+    };
+    auto bail = [&](mtx_status st) {
+        cleanup();
+        dev_free(c, mm);
+        dev_free(c, dv);
+        memset(out, 0, sizeof(*out));
+        return st;
+    };
+    cudaError_t e = cudaEventCreateWithFlags(&ready, cudaEventDisableTiming);
+    // the copies may start only after what the context's stream owes the new buffers
+    if (e == cudaSuccess) e = cudaEventRecord(ready, c->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->copy_stream, ready, 0);
+    for (uint32_t k = 0; k < nslab && e == cudaSuccess; ++k) {
+        const uint64_t z0 = (uint64_t)k * S * B, z1 = std::min<uint64_t>((uint64_t)(k + 1) * S * B, dims[2]);
+        e = cudaEventCreateWithFlags(&landed[k], cudaEventDisableTiming);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(static_cast<char *>(dv) + z0 * slice, static_cast<const char *>(host) + z0 * slice,
+                                (z1 - z0) * slice, cudaMemcpyHostToDevice, c->copy_stream);
+        if (e == cudaSuccess) e = cudaEventRecord(landed[k], c->copy_stream);
+    }
+    if (e != cudaSuccess) return bail(cuda_fail(c, e, "volume slab upload"));
+    prof_begin(prof, "MinMax_Leaf_Pass", c->stream);
+    for (uint32_t k = 0; k < nslab && r == MTX_OK; ++k) {
+        e = cudaStreamWaitEvent(c->stream, landed[std::min(k + 1, nslab - 1)], 0);
+        if (e != cudaSuccess) {
+            r = cuda_fail(c, e, "slab wait");
+            break;
+        }
+        const uint32_t b0 = k * S, b1 = std::min(p0.GZ, b0 + S);
+        Problem ps = p0;
+        ps.vol = static_cast<const char *>(dv) + (uint64_t)b0 * B * slice;
+        ps.Z = (uint32_t)(std::min<uint64_t>((uint64_t)b1 * B + 1, dims[2]) - (uint64_t)b0 * B);
+        ps.GZ = b1 - b0;
+        ps.nblocks = (uint64_t)p0.GX * p0.GY * ps.GZ;
+        r = launch_minmax_leaf(c, ps, (uint2 *)mm + (uint64_t)b0 * p0.GX * p0.GY, c->stream, 0);
+    }
+    prof_end(prof, c->stream);
+    if (r == MTX_OK && L > 1) {
+        prof_begin(prof, "MinMax_Octree_Reduction", c->stream);
+        r = launch_pyramid(c, (uint2 *)mm, L, out->levelExtent, out->levelOffset, c->stream, 0);
+        prof_end(prof, c->stream);
+    }
+    if (r != MTX_OK) return bail(r);
+    cleanup();  // events are released once their work completes
+    *vol_out = v;
+    out->volumeImage = v;
+    out->volumeImage.owned = 0;
+    out->minMaxImage.ptr = mm;
+    out->minMaxImage.size = total * sizeof(uint2);
+    out->mipLevels = (uint32_t)L;
+    for (int a = 0; a < 3; ++a) {
+        out->blockDim[a] = pc->blockDim[a];
+        out->blockGridDim[a] = grid[a];
+    }
+    return MTX_OK;
+}
+
 mtx_status mtx_minmax_free(mtx_context_t c, mtx_minmax_output *mm) {
     if (!c || !mm) return MTX_ERR_INVALID_ARG;
     DeviceGuard g(c->device);
-    cudaStreamSynchronize(c->stream);
-    dev_free(mm->minMaxImage.ptr);
+    dev_free(c, mm->minMaxImage.ptr);
     memset(mm, 0, sizeof(*mm));
     return MTX_OK;
 }
@@ -536,8 +686,8 @@ mtx_status mtx_filter_active_blocks(mtx_context_t c, const mtx_minmax_output *mm
     void *ids = nullptr, *cnt = nullptr, *rank = nullptr;
     if ((r = dev_alloc(c, &ids, p.nblocks * 4)) != MTX_OK) return r;
     if ((r = dev_alloc(c, &cnt, 4)) != MTX_OK || (r = dev_alloc(c, &rank, p.nblocks * 4)) != MTX_OK) {
-        dev_free(ids);
-        dev_free(cnt);
+        dev_free(c, ids);
+        dev_free(c, cnt);
         return r;
     }
     prof_begin(prof, "Active_Block_Filtering", c->stream);
@@ -545,9 +695,9 @@ mtx_status mtx_filter_active_blocks(mtx_context_t c, const mtx_minmax_output *mm
                       nullptr, c->stream);
     prof_end(prof, c->stream);
     if (r != MTX_OK) {
-        dev_free(ids);
-        dev_free(cnt);
-        dev_free(rank);
+        dev_free(c, ids);
+        dev_free(c, cnt);
+        dev_free(c, rank);
         return r;
     }
     out->compactedBlockIdBuffer = {ids, p.nblocks * 4};
@@ -583,10 +733,9 @@ mtx_status mtx_read_buffer(mtx_context_t c, const mtx_buffer *src, uint64_t offs
 mtx_status mtx_filtering_free(mtx_context_t c, mtx_filtering_output *f) {
     if (!c || !f) return MTX_ERR_INVALID_ARG;
     DeviceGuard g(c->device);
-    cudaStreamSynchronize(c->stream);
-    dev_free(f->compactedBlockIdBuffer.ptr);
-    dev_free(f->activeBlockCountBuffer.ptr);
-    dev_free(f->blockRankBuffer.ptr);
+    dev_free(c, f->compactedBlockIdBuffer.ptr);
+    dev_free(c, f->activeBlockCountBuffer.ptr);
+    dev_free(c, f->blockRankBuffer.ptr);
     memset(f, 0, sizeof(*f));
     return MTX_OK;
 }
@@ -623,14 +772,14 @@ mtx_status mtx_extract_meshlet_descriptors(mtx_context_t c, const mtx_minmax_out
     void *desc = nullptr, *counters = nullptr;
     if ((r = dev_alloc(c, &desc, (size_t)n * sizeof(mtx_meshlet_descriptor))) != MTX_OK) return r;
     if ((r = dev_alloc(c, &counters, 16)) != MTX_OK) {
-        dev_free(desc);
+        dev_free(c, desc);
         return r;
     }
     auto bail = [&](mtx_status s) {
-        dev_free(desc);
-        dev_free(counters);
-        dev_free(out->vertexBuffer.ptr);
-        dev_free(out->indexBuffer.ptr);
+        dev_free(c, desc);
+        dev_free(c, counters);
+        dev_free(c, out->vertexBuffer.ptr);
+        dev_free(c, out->indexBuffer.ptr);
         memset(out, 0, sizeof(*out));
         return s;
     };
@@ -695,11 +844,10 @@ mtx_status mtx_extract_meshlet_descriptors(mtx_context_t c, const mtx_minmax_out
 mtx_status mtx_extraction_free(mtx_context_t c, mtx_extraction_output *x) {
     if (!c || !x) return MTX_ERR_INVALID_ARG;
     DeviceGuard g(c->device);
-    cudaStreamSynchronize(c->stream);
-    dev_free(x->vertexBuffer.ptr);
-    dev_free(x->indexBuffer.ptr);
-    dev_free(x->meshletDescriptorBuffer.ptr);
-    dev_free(x->vertexCountBuffer.ptr);  // the three counters share one allocation
+    dev_free(c, x->vertexBuffer.ptr);
+    dev_free(c, x->indexBuffer.ptr);
+    dev_free(c, x->meshletDescriptorBuffer.ptr);
+    dev_free(c, x->vertexCountBuffer.ptr);  // the three counters share one allocation
     const uint32_t stride = x->vertexStride;
     memset(x, 0, sizeof(*x));
     x->vertexStride = stride;

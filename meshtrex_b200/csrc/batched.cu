@@ -647,7 +647,7 @@ void batch_release(mtx_batch *b) {
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
     if (b->capture_stream) cudaStreamDestroy(b->capture_stream);
-    for (void *p : b->allocs) dev_free(p);
+    for (void *p : b->allocs) dev_free(b->ctx, p);
     delete b;
 }
 

@@ -181,31 +181,68 @@ mtx_status launch_filter(mtx_context *c, const Problem &p, const uint2 *leaf, ui
 namespace mtx {
 constexpr uint32_t kNoallocMaxTiles = 65536;                // up to 65536 * 1024 = 67,108,864 blocks
 constexpr uint32_t kNoallocTicket = kNoallocMaxTiles;       // word index of the tile ticket
-constexpr uint32_t kNoallocStatus = kNoallocMaxTiles + 4;   // 4 words: error record if the caller passes none
-constexpr uint32_t kNoallocWords = kNoallocMaxTiles + 8;    // 256 KiB + 32 bytes
+constexpr uint32_t kNoallocWords = kNoallocMaxTiles + 64;   // 256 KiB + 256 bytes
 }  // namespace mtx
 
 // Words [0, ntiles) hold the look-back status of each tile, then the ticket
-// counter and a fallback error record.
+// counter.
 static __device__ __align__(256) uint32_t g_noalloc_scratch[mtx::kNoallocWords];
 
 namespace {
-// Device address of g_noalloc_scratch, looked up once per device (with that
-// device current).  Host code must not use the symbol itself as a pointer:
-// on the host it names a stand-in object, not device memory.
-uint32_t *g_noalloc_ptr[128] = {nullptr};
+// Device address of g_noalloc_scratch in the calling thread's current CUDA
+// context.  Host code must not use the symbol itself as a pointer: on the
+// host it names a stand-in object, not device memory.  The address belongs
+// to the context that loaded the module, so it is cached per context id
+// (cuCtxGetId, unique for the life of the process): after cudaDeviceReset,
+// or under another context on the same device, the next call looks it up
+// again instead of using a stale address.
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long *);
+struct NoallocSlot {
+    unsigned long long ctx_id;
+    uint32_t *ptr;
+};
+constexpr int kNoallocSlots = 64;
+NoallocSlot g_noalloc_slots[kNoallocSlots] = {};
+int g_noalloc_next = 0;
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CtxGetIdFn g_ctx_get_id = nullptr;
 std::mutex g_noalloc_mu;
 
 cudaError_t noalloc_scratch(int device, uint32_t **out) {
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (device < 0 || device >= 128) return cudaErrorInvalidDevice;
-    if (!g_noalloc_ptr[device]) {
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (!g_ctx_get_current || !g_ctx_get_id) {
+        void *f0 = nullptr, *f1 = nullptr;
+        cudaDriverEntryPointQueryResult q0, q1;
+        cudaError_t e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &f0, cudaEnableDefault, &q0);
         if (e != cudaSuccess) return e;
-        g_noalloc_ptr[device] = static_cast<uint32_t *>(p);
+        e = cudaGetDriverEntryPoint("cuCtxGetId", &f1, cudaEnableDefault, &q1);
+        if (e != cudaSuccess) return e;
+        if (q0 != cudaDriverEntryPointSuccess || q1 != cudaDriverEntryPointSuccess || !f0 || !f1)
+            return cudaErrorNotSupported;
+        g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(f0);
+        g_ctx_get_id = reinterpret_cast<CtxGetIdFn>(f1);
     }
-    *out = g_noalloc_ptr[device];
+    CUcontext cu = nullptr;
+    if (g_ctx_get_current(&cu) != CUDA_SUCCESS) return cudaErrorDeviceUninitialized;
+    if (!cu) {  // no context yet on this thread: bind the device's primary context, as a launch would
+        const cudaError_t e = cudaSetDevice(device);
+        if (e != cudaSuccess) return e;
+        if (g_ctx_get_current(&cu) != CUDA_SUCCESS || !cu) return cudaErrorDeviceUninitialized;
+    }
+    unsigned long long id = 0;
+    if (g_ctx_get_id(cu, &id) != CUDA_SUCCESS) return cudaErrorDeviceUninitialized;
+    for (const NoallocSlot &s : g_noalloc_slots)
+        if (s.ptr && s.ctx_id == id) {
+            *out = s.ptr;
+            return cudaSuccess;
+        }
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    g_noalloc_slots[g_noalloc_next] = {id, static_cast<uint32_t *>(p)};
+    g_noalloc_next = (g_noalloc_next + 1) % kNoallocSlots;
+    *out = static_cast<uint32_t *>(p);
     return cudaSuccess;
 }
 }  // namespace
@@ -215,7 +252,13 @@ extern "C" mtx_status mtx_filter_active_blocks_noalloc(const uint32_t *leaf_minm
                                                        uint32_t *block_rank, uint32_t *active_count,
                                                        uint32_t *device_status, void *stream) {
     using namespace mtx;
-    if (!leaf_minmax || !compacted_ids || !block_rank || !active_count || dtype > MTX_DTYPE_F32 || total_blocks == 0)
+    if (!leaf_minmax || !compacted_ids || !block_rank || !active_count || !device_status ||
+        dtype > MTX_DTYPE_F32 || total_blocks == 0)
+        return MTX_ERR_INVALID_ARG;
+    // the kernel reads the keys and writes the ranks as 16-byte words
+    if ((reinterpret_cast<uintptr_t>(leaf_minmax) | reinterpret_cast<uintptr_t>(block_rank)) % 16 != 0 ||
+        reinterpret_cast<uintptr_t>(compacted_ids) % 4 != 0 || reinterpret_cast<uintptr_t>(active_count) % 4 != 0 ||
+        reinterpret_cast<uintptr_t>(device_status) % 4 != 0)
         return MTX_ERR_INVALID_ARG;
     if (total_blocks > (uint64_t)kNoallocMaxTiles * kNoallocTile) return MTX_ERR_CAPACITY;
     const uint32_t ntiles = (uint32_t)((total_blocks + kNoallocTile - 1) / kNoallocTile);
@@ -230,15 +273,12 @@ extern "C" mtx_status mtx_filter_active_blocks_noalloc(const uint32_t *leaf_minm
         return MTX_ERR_CUDA;
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    DevStatus *st = reinterpret_cast<DevStatus *>(device_status ? device_status : sc + kNoallocStatus);
+    DevStatus *st = reinterpret_cast<DevStatus *>(device_status);
     // the array keeps the previous call's contents: clear what must start at zero
     if (cudaMemsetAsync(sc, 0, sizeof(uint32_t) * (size_t)ntiles, s) != cudaSuccess ||
         cudaMemsetAsync(sc + kNoallocTicket, 0, sizeof(uint32_t), s) != cudaSuccess ||
-        cudaMemsetAsync(active_count, 0, sizeof(uint32_t), s) != cudaSuccess) {
-        cudaGetLastError();
-        return MTX_ERR_CUDA;
-    }
-    if (device_status && cudaMemsetAsync(device_status, 0, sizeof(DevStatus), s) != cudaSuccess) {
+        cudaMemsetAsync(active_count, 0, sizeof(uint32_t), s) != cudaSuccess ||
+        cudaMemsetAsync(device_status, 0, sizeof(DevStatus), s) != cudaSuccess) {
         cudaGetLastError();
         return MTX_ERR_CUDA;
     }

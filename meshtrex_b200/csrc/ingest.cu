@@ -72,7 +72,7 @@ mtx_status mtx_volume_load(mtx_context_t c, const char *path, mtx_volume *out) {
             if (done[i]) cudaEventDestroy(done[i]);
             if (stage[i]) cudaFreeHost(stage[i]);
         }
-        if (!keep) dev_free(dev);
+        if (!keep) dev_free(c, dev);
     };
     for (int i = 0; i < 2; ++i) {
         cudaError_t e = cudaHostAlloc(&stage[i], chunk, cudaHostAllocDefault);

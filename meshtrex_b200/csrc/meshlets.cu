@@ -129,8 +129,8 @@ extern "C" mtx_status mtx_build_meshlets(mtx_context_t c, const mtx_extraction_o
     mtx_status r;
     if ((r = dev_alloc(c, &per_block, sizeof(mtx_meshlet_descriptor) * (size_t)nb)) != MTX_OK) return r;
     auto bail = [&](mtx_status st) {
-        dev_free(per_block);
-        dev_free(counters);
+        dev_free(c, per_block);
+        dev_free(c, counters);
         mtx_meshlet_output_free(c, out);
         return st;
     };
@@ -171,8 +171,8 @@ extern "C" mtx_status mtx_build_meshlets(mtx_context_t c, const mtx_extraction_o
                                                                (const uint32_t *)p_mv, MV, stride, (float *)p_vd);
     if ((e = cudaGetLastError()) != cudaSuccess) return bail(cuda_fail(c, e, "meshlet gather launch"));
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return bail(cuda_fail(c, e, "meshlet build"));
-    dev_free(per_block);
-    dev_free(counters);
+    dev_free(c, per_block);
+    dev_free(c, counters);
     out->meshletCount = M;
     out->vertexCount = MV;
     out->indexCount = 3u * T;
@@ -182,11 +182,10 @@ extern "C" mtx_status mtx_build_meshlets(mtx_context_t c, const mtx_extraction_o
 extern "C" mtx_status mtx_meshlet_output_free(mtx_context_t c, mtx_meshlet_output *out) {
     if (!c || !out) return MTX_ERR_INVALID_ARG;
     DeviceGuard dg(c->device);
-    cudaStreamSynchronize(c->stream);
-    dev_free(out->meshletDescriptorBuffer.ptr);
-    dev_free(out->meshletVertexBuffer.ptr);
-    dev_free(out->vertexBuffer.ptr);
-    dev_free(out->indexBuffer.ptr);
+    dev_free(c, out->meshletDescriptorBuffer.ptr);
+    dev_free(c, out->meshletVertexBuffer.ptr);
+    dev_free(c, out->vertexBuffer.ptr);
+    dev_free(c, out->indexBuffer.ptr);
     const uint32_t stride = out->vertexStride;
     memset(out, 0, sizeof(*out));
     out->vertexStride = stride;

@@ -48,6 +48,7 @@ struct mtx_context {
     mtx::Scratch adj_partial, adj_iso;  // adjoint: per-block partial tiles and isovalue sums
     mtx_profiler *prof = nullptr;  // records stage times of calls given no profiler
     mtx_tuning tuning = {0, 0, 0, 0};
+    cudaStream_t copy_stream = nullptr;  // host-to-device slabs of mtx_upload_compute_min_max_mip (made on first use)
 };
 
 namespace mtx {
@@ -74,7 +75,7 @@ mtx_status cuda_fail(mtx_context *c, cudaError_t e, const char *what);
     } while (0)
 
 mtx_status dev_alloc(mtx_context *c, void **p, size_t bytes);
-void dev_free(void *p);
+void dev_free(mtx_context *c, void *p);  // ordered on c's stream (c may be null: a device-wide wait)
 mtx_status scratch_reserve(mtx_context *c, Scratch &s, size_t bytes);
 
 inline uint32_t dtype_size(uint32_t dt) { return dt == MTX_DTYPE_U8 ? 1u : dt == MTX_DTYPE_U16 ? 2u : 4u; }

@@ -36,11 +36,20 @@ class _Counts(C.Structure):
 _lib = None
 
 
+def reference_src() -> str | None:
+    """meshtrex's src directory: $REFERENCE_SRC, else a meshtrex checkout named
+    "reference" beside this repository; None when neither holds testMinMax.h."""
+    cand = os.environ.get("REFERENCE_SRC") or os.path.join(HERE, "..", "..", "reference", "src")
+    cand = os.path.abspath(cand)
+    return cand if os.path.isfile(os.path.join(cand, "testMinMax.h")) else None
+
+
 def build() -> None:
     """Compile liboracle.so (and the reference harness when the reference tree exists)."""
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
-    if os.path.isdir(os.environ.get("REFERENCE_SRC", "/root/reference/src")):
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+    src = reference_src()
+    if src:
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE_SRC={src}"], check=True)
 
 
 def lib():

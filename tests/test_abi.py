@@ -87,3 +87,20 @@ def test_tensor_map_plan_alignment():
             for bx in range(64):
                 ox = bx * B
                 assert ox % A <= xoff_max and ox % A + B + 1 <= PX
+
+
+def test_noalloc_compaction_rejects_bad_pointers_before_any_work():
+    """mtx_filter_active_blocks_noalloc checks its arguments before it touches
+    the GPU: the status record is required, and the keys and the rank map are
+    read and written as 16-byte words, so they must be 16-byte aligned.  The
+    pointers below are never dereferenced."""
+    from meshtrex_b200 import _lib as L
+    f = L.lib().mtx_filter_active_blocks_noalloc
+    ok = C.c_void_p(0x10000)
+    off8 = C.c_void_p(0x10008)
+    assert f(ok, 16, L.DTYPE_U8, 1.0, ok, ok, ok, None, None) == 1      # no status record
+    assert f(off8, 16, L.DTYPE_U8, 1.0, ok, ok, ok, ok, None) == 1      # keys not 16-byte aligned
+    assert f(ok, 16, L.DTYPE_U8, 1.0, ok, off8, ok, ok, None) == 1      # rank map not 16-byte aligned
+    assert f(ok, 16, 3, 1.0, ok, ok, ok, ok, None) == 1                 # unknown dtype
+    assert f(ok, 0, L.DTYPE_U8, 1.0, ok, ok, ok, ok, None) == 1         # no blocks
+    assert f(ok, 65536 * 1024 + 1, L.DTYPE_U8, 1.0, ok, ok, ok, ok, None) == 4  # beyond the array

@@ -59,3 +59,20 @@ def test_reference_arm_prints_only_on_rank_zero():
     r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2"],
                        capture_output=True, text=True, env=env, timeout=300)
     assert r.returncode == 0 and r.stdout.strip() == ""
+
+
+def test_gpus_two_starts_two_ranks_and_reports_two():
+    """`bench.py --gpus 2` run directly (no torchrun around it) starts two ranks
+    under torchrun itself; on the reference arm rank 0 alone prints, with
+    n_gpus 2, and the other rank exits 0 without work.  A 64^3 volume keeps the
+    CPU work to a second."""
+    import json
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "LOCAL_RANK", "WORLD_SIZE", "MASTER_ADDR",
+                                                            "MASTER_PORT")}
+    r = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--gpus", "2",
+                        "--size", "64", "--steps", "1", "--warmup", "3"],
+                       capture_output=True, text=True, env=env, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [json.loads(l) for l in r.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1
+    assert lines[0]["n_gpus"] == 2 and lines[0]["impl"] == "reference"

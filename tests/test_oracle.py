@@ -206,3 +206,23 @@ def test_meshlet_rule_on_a_hand_mesh(oracle):
     np.testing.assert_array_equal(mv[mi], idx)
     d2, _, _ = oracle.meshlets(nt, idx, 64, 1)  # one triangle per meshlet
     assert len(d2) == 5 and (d2[:, 3] == 1).all()
+
+
+# ------------------------------------------------- meshtrex's sphere fixture
+def test_sphere_fixture_bytes_are_pinned():
+    """sphere_volume restates generateSphereVolume (src/meshtrex.cpp:23-52);
+    its bytes are pinned, and both readings of the unqualified sqrt there
+    (float overload, or double sqrt and subtraction rounded once) agree."""
+    from golden.fixtures import sphere_volume
+    pins = json.load(open(os.path.join(HERE, "golden", "fixture_pins.json")))
+    v = sphere_volume()
+    assert v.shape == (64, 64, 64) and v.dtype == np.uint8
+    assert sha(v) == pins["sphere_64_sha256"]
+    f = np.float32
+    radius = f(64) * f(0.4)
+    z, y, x = np.meshgrid(*(np.arange(64, dtype=f),) * 3, indexing="ij")
+    dx, dy, dz = x - f(32), y - f(32), z - f(32)
+    s = (dx * dx + dy * dy) + dz * dz
+    dist = (np.sqrt(s.astype(np.float64)) - np.float64(radius)).astype(f)
+    n = ((dist / radius) * f(127.0) + f(128.0)) + f(0.001)
+    np.testing.assert_array_equal(np.maximum(f(0), np.minimum(f(255), n)).astype(np.uint8), v)

@@ -79,7 +79,51 @@ def test_noalloc_rejects_sizes_beyond_its_array():
     from meshtrex_b200 import _lib as L
     dummy = torch.zeros(4, dtype=torch.int32, device="cuda")
     p = C.c_void_p(dummy.data_ptr())
-    rc = L.lib().mtx_filter_active_blocks_noalloc(p, 65536 * 1024 + 1, L.DTYPE_U8, 1.0, p, p, p, None, None)
+    rc = L.lib().mtx_filter_active_blocks_noalloc(p, 65536 * 1024 + 1, L.DTYPE_U8, 1.0, p, p, p, p, None)
     assert rc == 4  # MTX_ERR_CAPACITY, before any GPU work
-    rc = L.lib().mtx_filter_active_blocks_noalloc(None, 16, L.DTYPE_U8, 1.0, p, p, p, None, None)
+    rc = L.lib().mtx_filter_active_blocks_noalloc(None, 16, L.DTYPE_U8, 1.0, p, p, p, p, None)
     assert rc == 1  # MTX_ERR_INVALID_ARG
+
+
+def _build_context_program(out_dir):
+    """tests/cpp/noalloc_contexts.cpp, linked against the library and the CUDA
+    driver (the link-time stub; the driver itself is loaded at run time)."""
+    import os
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    lib_dir = os.path.join(root, "meshtrex_b200")
+    cuda = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+    exe = os.path.join(str(out_dir), "noalloc_contexts")
+    cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-Werror", "-I", os.path.join(root, "include"),
+           "-I", os.path.join(cuda, "include"), os.path.join(root, "tests", "cpp", "noalloc_contexts.cpp"),
+           "-L", lib_dir, "-lmeshtrex_b200", f"-Wl,-rpath,{lib_dir}", "-L", os.path.join(cuda, "lib64", "stubs"),
+           "-lcuda", "-o", exe]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    return exe
+
+
+def test_noalloc_in_a_second_cuda_context(tmp_path, oracle):
+    """The scratch array's device address belongs to a CUDA context: a call in
+    a second context on the same device must look it up there, and a later
+    call in the first context must still use the first one's."""
+    import json
+    import subprocess
+    a = blob_volume((40, 56, 64), np.uint8, seed=23)
+    keys = oracle.minmax_halo(a, 4)  # 10 x 14 x 16 = 2240 blocks: three 1024-block tiles
+    iso = 128.5
+    path = tmp_path / "keys.bin"
+    keys.astype(np.uint32).tofile(path)
+    exe = _build_context_program(tmp_path)
+    r = subprocess.run([exe, str(path), "0", repr(iso)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0, r.stderr
+    calls = json.loads(r.stdout.strip().splitlines()[-1])["calls"]
+    ids = oracle.compact(keys, oracle.U8, iso)
+    rank = np.full(keys.shape[0], 0xFFFFFFFF, np.uint32)
+    rank[ids] = np.arange(len(ids), dtype=np.uint32)
+    from test_gpu_facade import _fnv1a
+    want = {"status": 0, "count": len(ids), "device_status": 0, "ids": _fnv1a(ids.astype(np.uint32).tobytes()),
+            "rank": _fnv1a(rank.tobytes())}
+    assert len(ids) > 0
+    for c in calls:
+        assert c == want
