@@ -496,73 +496,73 @@ def load_or_make_volume(cache):
 
 
 def run_e2e(ctx, vol_dev, ws, steps):
-    """The drop-in C-ABI path from pinned host memory, per extraction: upload
-    (mtx_volume_upload), computeMinMaxMip, filterActiveBlocks,
-    readActiveBlockCount, extractMeshletDescriptors, and the mesh read back to
-    pinned host buffers.  The step's three extractions run on three contexts,
-    each with its own stream: the three uploads are enqueued first, so that
-    while later volumes still cross PCIe the earlier ones are extracted and
-    their meshes copied back.  One untimed step warms the allocations."""
-    import ctypes as C
-
-    from meshtrex_b200 import _lib as L
+    """The drop-in C-ABI path from pinned host memory.  Each step takes its
+    input volume from pinned host memory once, with
+    mtx_upload_compute_min_max_mip (z-slabs on a copy stream, the first
+    extraction's leaf min/max consuming each slab as it lands), then runs the
+    three extractions through computeMinMaxMip (the second and third, on the
+    resident volume), filterActiveBlocks, readActiveBlockCount and
+    extractMeshletDescriptors, and copies every mesh to pinned host memory.
+    Two contexts alternate between steps: step k + 1's upload is enqueued when
+    step k begins, so that it crosses PCIe while step k is extracted and read
+    back.  One untimed step warms the allocations."""
     from meshtrex_b200 import api
-    host = torch.empty(vol_dev.shape, dtype=vol_dev.dtype, pin_memory=True)
-    host.copy_(vol_dev)
-    dims = (C.c_uint32 * 3)(N, N, N)
+    t = torch.empty(vol_dev.numel() * vol_dev.element_size(), dtype=torch.uint8, pin_memory=True)
+    t.copy_(vol_dev.view(torch.uint8).reshape(-1))
+    host = t.numpy().view(np.uint16).reshape(N, N, N)
     local = torch.cuda.current_device()
-    streams = [torch.cuda.Stream() for _ in ISOS]
+    streams = [torch.cuda.Stream() for _ in range(2)]
     ctxs = [api.Context(local, stream=s_) for s_ in streams]
     out_v = [torch.empty(1, dtype=torch.float32, pin_memory=True) for _ in ISOS]
     out_i = [torch.empty(1, dtype=torch.int32, pin_memory=True) for _ in ISOS]
+    pcs = [api.push_constants((N, N, N), BLOCK, iso) for iso in ISOS]
 
-    def step():
-        h2d = d2h = 0
-        vols, live = [], []
-        for c_ in ctxs:  # every upload first: they queue on the copy engine
-            v = L.Volume()
-            L.check(L.lib().mtx_volume_upload(c_.handle, C.c_void_p(host.data_ptr()), dims, L.DTYPE_U16,
-                                              C.byref(v)), "upload", c_.handle)
-            vols.append(v)
-            h2d += v.data.size
-        for k, (c_, s_, v, iso) in enumerate(zip(ctxs, streams, vols, ISOS)):
-            pc = api.push_constants((N, N, N), BLOCK, iso)
-            mm = api.compute_min_max_mip(c_, v, pc)
+    def upload(k):
+        c_ = ctxs[k % 2]
+        return api.upload_compute_min_max_mip(c_, host, pcs[0])
+
+    def extract_step(k, v, mm0, prefetch):
+        c_, s_ = ctxs[k % 2], streams[k % 2]
+        nxt = upload(k + 1) if prefetch else None
+        h2d, d2h, live = v.data.size, 0, []
+        for j, pc in enumerate(pcs):
+            mm = mm0 if j == 0 else api.compute_min_max_mip(c_, v, pc)
             f = api.filter_active_blocks(c_, mm, pc)
             api.read_active_block_count(c_, f)
             x = api.extract_meshlet_descriptors(c_, mm, f, pc)
             nv, ni = x.out.vertexBuffer.size, x.out.indexBuffer.size
-            if out_v[k].numel() * 4 < nv:
-                out_v[k] = torch.empty(nv // 4 + 1, dtype=torch.float32, pin_memory=True)
-            if out_i[k].numel() * 4 < ni:
-                out_i[k] = torch.empty(ni // 4 + 1, dtype=torch.int32, pin_memory=True)
-            # device -> pinned host copies of the mesh, on the extraction's stream
-            with torch.cuda.stream(s_):
+            if out_v[j].numel() * 4 < nv:
+                out_v[j] = torch.empty(nv // 4 + 1, dtype=torch.float32, pin_memory=True)
+            if out_i[j].numel() * 4 < ni:
+                out_i[j] = torch.empty(ni // 4 + 1, dtype=torch.int32, pin_memory=True)
+            with torch.cuda.stream(s_):  # device -> pinned host copies of the mesh, on the extraction's stream
                 if nv:
-                    out_v[k][: nv // 4].copy_(api.device_view(x.out.vertexBuffer.ptr, (nv // 4,), torch.float32),
+                    out_v[j][: nv // 4].copy_(api.device_view(x.out.vertexBuffer.ptr, (nv // 4,), torch.float32),
                                               non_blocking=True)
                 if ni:
-                    out_i[k][: ni // 4].copy_(api.device_view(x.out.indexBuffer.ptr, (ni // 4,), torch.int32),
+                    out_i[j][: ni // 4].copy_(api.device_view(x.out.indexBuffer.ptr, (ni // 4,), torch.int32),
                                               non_blocking=True)
             d2h += nv + ni
-            live.append((c_, v, mm, f, x))
-        torch.cuda.synchronize()
-        for c_, v, mm, f, x in live:
+            live.append((mm, f, x))
+        s_.synchronize()  # the step's meshes are on the host
+        for mm, f, x in live:
             x.free()
             f.free()
             mm.free()
-            L.lib().mtx_volume_free(c_.handle, C.byref(v))
-        return h2d, d2h
+        api.free_volume(c_, v)
+        return nxt, h2d, d2h
 
-    step()  # untimed
+    nxt = upload(0)
+    extract_step(0, *nxt, prefetch=False)  # untimed
     torch.cuda.synchronize()
     if ws > 1:
         import torch.distributed as dist
         dist.barrier()
     h2d = d2h = 0
     t0 = time.perf_counter()
-    for _ in range(steps):
-        a_, b_ = step()
+    cur = upload(0)
+    for k in range(steps):
+        cur, a_, b_ = extract_step(k, *cur, prefetch=k + 1 < steps)
         h2d += a_
         d2h += b_
     torch.cuda.synchronize()
@@ -571,9 +571,11 @@ def run_e2e(ctx, vol_dev, ws, steps):
         c_.close()
     return {"value": job_throughput(3 * N ** 3 * steps, ws, t) / 1e9, "unit": "Gvoxels/s",
             "h2d_bytes_per_step": h2d // steps, "d2h_bytes_per_step": d2h // steps, "steps": steps,
-            "what": "per extraction: mtx_volume_upload from pinned host memory -> computeMinMaxMip -> "
-                    "filterActiveBlocks -> readActiveBlockCount -> extractMeshletDescriptors -> mesh copied "
-                    "to pinned host memory; the step's three extractions on three streams, uploads enqueued first"}
+            "what": "per step: the volume from pinned host memory once (mtx_upload_compute_min_max_mip, z-slabs "
+                    "with the first extraction's leaf min/max overlapped), then per isovalue computeMinMaxMip -> "
+                    "filterActiveBlocks -> readActiveBlockCount -> extractMeshletDescriptors -> mesh copied to "
+                    "pinned host memory; two contexts alternate so that the next step's upload overlaps this "
+                    "step's extractions"}
 
 
 def run_batched(ctx, stream, steps, scale_down=1):

@@ -197,6 +197,18 @@ uint32_t mtx_abi_version(void);
 mtx_status mtx_context_create(int device, void *stream, mtx_context_t *out);
 mtx_status mtx_context_destroy(mtx_context_t ctx);
 mtx_status mtx_context_set_stream(mtx_context_t ctx, void *stream);
+/* A second stream for the count, scan and emit passes of
+ * mtx_extract_plain_async (NULL: none, everything on the context's stream).
+ * With it, the call queues the leaf min/max, octree and filter on the
+ * context's stream and the extraction passes on this one behind an event, so
+ * that work queued next on the context's stream -- the min/max of the next
+ * volume or isovalue, for one -- runs while this extraction is still being
+ * emitted.  The context's scratch is reused by its next call, so that call's
+ * filter waits for this extraction first, and every other call on the context
+ * joins the extraction stream before it starts.  mtx_synchronize waits for
+ * both streams.  Meant for eager use: a stream capture must not span calls on
+ * such a context.  No meshtrex counterpart (one queue, vulkan_context.cpp:94-109). */
+mtx_status mtx_context_set_extract_stream(mtx_context_t ctx, void *stream);
 /* Last error text of this context ("" if none). */
 const char *mtx_context_last_error(mtx_context_t ctx);
 /* Wait for the stream, then report (and clear) any error a kernel recorded. */
@@ -506,6 +518,8 @@ typedef struct mtx_tuning {
                                1, 2 or 4: the load-based pass with that many z slices in flight */
     uint32_t extractWarps;  /* warps per CTA of the extraction passes: 1, 2, 4 (default) or 8 */
     uint32_t staging;       /* mtx_staging used when the extract options say AUTO */
+    uint32_t extractCtasPerSm; /* at most this many CTAs an SM in the count and emit passes (0 = as many as
+                                  fit): leaves room on each SM for another stream's min/max pass */
 } mtx_tuning;
 mtx_status mtx_context_set_tuning(mtx_context_t ctx, const mtx_tuning *t);
 mtx_status mtx_context_get_tuning(mtx_context_t ctx, mtx_tuning *t);

@@ -79,7 +79,7 @@ class ExtractionOutput(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("minmaxZChunk", C.c_uint32), ("minmaxSlices", C.c_uint32),
-                ("extractWarps", C.c_uint32), ("staging", C.c_uint32)]
+                ("extractWarps", C.c_uint32), ("staging", C.c_uint32), ("extractCtasPerSm", C.c_uint32)]
 
 
 class MeshBuffers(C.Structure):
@@ -146,6 +146,7 @@ SIGNATURES = [
     ("mtx_context_create", _ST, [C.c_int, _P, C.POINTER(_P)]),
     ("mtx_context_destroy", _ST, [_P]),
     ("mtx_context_set_stream", _ST, [_P, _P]),
+    ("mtx_context_set_extract_stream", _ST, [_P, _P]),
     ("mtx_context_last_error", C.c_char_p, [_P]),
     ("mtx_synchronize", _ST, [_P]),
     ("mtx_debug_fail_allocation", _ST, [_P, C.c_uint32]),

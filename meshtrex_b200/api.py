@@ -52,12 +52,25 @@ class Context:
 
     def __init__(self, device: int = 0, stream=None):
         self.handle = C.c_void_p()
-        L.check(L.lib().mtx_context_create(device, C.c_void_p(_stream_ptr(stream)),
+        self.stream_ptr = _stream_ptr(stream)
+        L.check(L.lib().mtx_context_create(device, C.c_void_p(self.stream_ptr),
                                            C.byref(self.handle)), "mtx_context_create")
 
     def set_stream(self, stream=None):
-        L.check(L.lib().mtx_context_set_stream(self.handle, C.c_void_p(_stream_ptr(stream))),
+        self.stream_ptr = _stream_ptr(stream)
+        L.check(L.lib().mtx_context_set_stream(self.handle, C.c_void_p(self.stream_ptr)),
                 "mtx_context_set_stream", self.handle)
+
+    def fence(self):
+        """Orders the context's stream after torch's current stream.  The
+        library frees in the order of its own stream, so work queued on the
+        current stream that reads a library buffer (the copies the accessors
+        below make) must come first; the *.free() methods call this."""
+        cur = torch.cuda.current_stream()
+        if int(cur.cuda_stream) != self.stream_ptr:
+            ev = torch.cuda.Event()
+            ev.record(cur)
+            torch.cuda.ExternalStream(self.stream_ptr).wait_event(ev)
 
     def synchronize(self):
         L.check(L.lib().mtx_synchronize(self.handle), "mtx_synchronize", self.handle)
@@ -66,8 +79,16 @@ class Context:
         L.check(L.lib().mtx_context_set_profiler(self.handle, prof.handle if prof else None),
                 "mtx_context_set_profiler")
 
-    def set_tuning(self, minmax_zchunk=0, minmax_slices=0, extract_warps=0, staging=0):
-        t = L.Tuning(minmax_zchunk, minmax_slices, extract_warps, staging)
+    def set_extract_stream(self, stream=None):
+        """Count, scan and emit of AsyncExtractor.run on `stream` (None: the
+        context's own stream), so that the next work on the context's stream
+        overlaps them (mtx_context_set_extract_stream)."""
+        ptr = int(stream.cuda_stream) if stream is not None else 0
+        L.check(L.lib().mtx_context_set_extract_stream(self.handle, C.c_void_p(ptr)),
+                "mtx_context_set_extract_stream", self.handle)
+
+    def set_tuning(self, minmax_zchunk=0, minmax_slices=0, extract_warps=0, staging=0, extract_ctas_per_sm=0):
+        t = L.Tuning(minmax_zchunk, minmax_slices, extract_warps, staging, extract_ctas_per_sm)
         L.check(L.lib().mtx_context_set_tuning(self.handle, C.byref(t)), "mtx_context_set_tuning",
                 self.handle)
 
@@ -126,6 +147,7 @@ def upload_volume(ctx: Context, a: np.ndarray) -> L.Volume:
 
 
 def free_volume(ctx: Context, v: L.Volume):
+    ctx.fence()
     L.lib().mtx_volume_free(ctx.handle, C.byref(v))
 
 
@@ -150,6 +172,7 @@ class MinMax:
 
     def free(self):
         if self.out.minMaxImage.ptr:
+            self.ctx.fence()
             L.lib().mtx_minmax_free(self.ctx.handle, C.byref(self.out))
 
 
@@ -171,6 +194,7 @@ class Filtering:
 
     def free(self):
         if self.out.compactedBlockIdBuffer.ptr:
+            self.ctx.fence()
             L.lib().mtx_filtering_free(self.ctx.handle, C.byref(self.out))
 
 
@@ -208,6 +232,7 @@ class Extraction:
 
     def free(self):
         if self.out.vertexCountBuffer.ptr or self.out.meshletDescriptorBuffer.ptr:
+            self.ctx.fence()
             L.lib().mtx_extraction_free(self.ctx.handle, C.byref(self.out))
 
 
@@ -347,6 +372,7 @@ def build_meshlets(ctx: Context, x: Extraction, max_vertices: int = 64, max_prim
                  device_view(o.meshletVertexBuffer.ptr, (o.vertexCount,), torch.int32).clone(),
                  device_view(o.vertexBuffer.ptr, (o.vertexCount, w), torch.float32).clone(),
                  device_view(o.indexBuffer.ptr, (o.indexCount // 3, 3), torch.int32).clone())
+    ctx.fence()
     L.lib().mtx_meshlet_output_free(ctx.handle, C.byref(o))
     return m
 
@@ -478,6 +504,7 @@ class Batch:
 
     def close(self):
         if self.handle:
+            self.ctx.fence()
             L.lib().mtx_batch_destroy(self.handle)
             self.handle = C.c_void_p()
 

@@ -192,6 +192,7 @@ extern "C" mtx_status mtx_extract_backward(mtx_context_t c, const mtx_volume *vo
                                            uint32_t frame, float *dl_dfield, float *dl_diso, uint32_t mode) {
     if (!c) return MTX_ERR_INVALID_ARG;
     DeviceGuard dg(c->device);
+    join_extract(c);
     if (!vol || !pc || !filt || !dl_dfield || !dl_diso) return fail(c, MTX_ERR_INVALID_ARG, "null argument");
     if (mode > MTX_ADJOINT_DETERMINISTIC || frame > MTX_FRAME_NDC || vertexStride < 3)
         return fail(c, MTX_ERR_INVALID_ARG, "bad adjoint mode, frame or vertex stride");

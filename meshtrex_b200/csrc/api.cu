@@ -216,8 +216,10 @@ void dev_free(mtx_context *c, void *p) {
 
 mtx_status scratch_reserve(mtx_context *c, Scratch &s, size_t bytes) {
     if (s.size >= bytes && s.ptr) return MTX_OK;
-    // grow geometrically; the old block is released in the order of the stream
+    // grow; the old block is released in the order of the stream, after any
+    // extraction still reading it on the extraction stream
     if (s.ptr) {
+        join_extract(c);
         dev_free(c, s.ptr);
         s.ptr = nullptr;
         s.size = 0;
@@ -226,6 +228,13 @@ mtx_status scratch_reserve(mtx_context *c, Scratch &s, size_t bytes) {
     mtx_status r = dev_alloc(c, &s.ptr, want);
     if (r != MTX_OK) return r;
     s.size = want;
+    return MTX_OK;
+}
+
+mtx_status join_extract(mtx_context *c) {
+    if (!c || !c->extract_pending) return MTX_OK;
+    c->extract_pending = false;
+    MTX_CUDA(c, cudaStreamWaitEvent(c->stream, c->ev_extracted, 0));
     return MTX_OK;
 }
 
@@ -421,12 +430,15 @@ mtx_status mtx_context_create(int device, void *stream, mtx_context_t *out) {
 mtx_status mtx_context_destroy(mtx_context_t c) {
     if (!c) return MTX_ERR_INVALID_ARG;
     DeviceGuard g(c->device);
+    join_extract(c);
     cudaStreamSynchronize(c->stream);
     for (Scratch *s : {&c->filter_status, &c->count_status, &c->faces, &c->state, &c->leaf, &c->ids, &c->rank,
                        &c->desc, &c->misc, &c->adj_partial, &c->adj_iso})
         dev_free(c, s->ptr);
     dev_cache_release(c->device);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+    if (c->ev_filtered) cudaEventDestroy(c->ev_filtered);
+    if (c->ev_extracted) cudaEventDestroy(c->ev_extracted);
     cudaFree(c->ctrl);
     cudaFreeHost(c->pinned);
     delete c;
@@ -435,7 +447,21 @@ mtx_status mtx_context_destroy(mtx_context_t c) {
 
 mtx_status mtx_context_set_stream(mtx_context_t c, void *stream) {
     if (!c) return MTX_ERR_INVALID_ARG;
+    DeviceGuard g(c->device);
     c->stream = (cudaStream_t)stream;
+    return join_extract(c);  // the new stream waits for an extraction still in flight
+}
+
+mtx_status mtx_context_set_extract_stream(mtx_context_t c, void *stream) {
+    if (!c) return MTX_ERR_INVALID_ARG;
+    DeviceGuard g(c->device);
+    join_extract(c);
+    if (stream && !c->ev_filtered) {
+        MTX_CUDA(c, cudaEventCreateWithFlags(&c->ev_filtered, cudaEventDisableTiming));
+        MTX_CUDA(c, cudaEventCreateWithFlags(&c->ev_extracted, cudaEventDisableTiming));
+    }
+    c->xstream = (cudaStream_t)stream;
+    c->has_xstream = stream != nullptr;
     return MTX_OK;
 }
 
@@ -444,6 +470,7 @@ const char *mtx_context_last_error(mtx_context_t c) { return c ? c->last_error.c
 mtx_status mtx_synchronize(mtx_context_t c) {
     if (!c) return MTX_ERR_INVALID_ARG;
     DeviceGuard g(c->device);
+    join_extract(c);
     MTX_CUDA(c, cudaStreamSynchronize(c->stream));
     return check_device_status(c);
 }
@@ -460,6 +487,7 @@ mtx_status mtx_volume_upload(mtx_context_t c, const void *host, const uint32_t d
     if (!c || !host || !dims || !out) return c ? fail(c, MTX_ERR_INVALID_ARG, "null argument") : MTX_ERR_INVALID_ARG;
     if (dtype > MTX_DTYPE_F32 || !dims[0] || !dims[1] || !dims[2]) return fail(c, MTX_ERR_INVALID_ARG, "bad volume");
     DeviceGuard g(c->device);
+    join_extract(c);
     const uint64_t bytes = nvox(dims) * dtype_size(dtype);
     void *d = nullptr;
     mtx_status r = dev_alloc(c, &d, bytes);
@@ -493,6 +521,7 @@ mtx_status mtx_volume_wrap(void *device_ptr, const uint32_t dims[3], uint32_t dt
 mtx_status mtx_volume_free(mtx_context_t c, mtx_volume *v) {
     if (!c || !v) return MTX_ERR_INVALID_ARG;
     DeviceGuard g(c->device);
+    join_extract(c);
     if (v->owned && v->data.ptr) dev_free(c, v->data.ptr);
     memset(v, 0, sizeof(*v));
     return MTX_OK;
@@ -522,6 +551,7 @@ mtx_status mtx_compute_min_max_mip(mtx_context_t c, const mtx_volume *vol, const
     if (r != MTX_OK) return r;
     if ((r = check_pc(c, vol, pc)) != MTX_OK) return r;
     DeviceGuard g(c->device);
+    join_extract(c);
     memset(out, 0, sizeof(*out));
     const Problem p = make_problem(vol, pc->blockDim[0], pc->isovalue);
     const uint32_t grid[3] = {p.GX, p.GY, p.GZ};
@@ -573,6 +603,7 @@ mtx_status mtx_upload_compute_min_max_mip(mtx_context_t c, const void *host, con
     if (dtype > MTX_DTYPE_F32 || !dims[0] || !dims[1] || !dims[2]) return fail(c, MTX_ERR_INVALID_ARG, "bad volume");
     if (!prof) prof = c->prof;
     DeviceGuard g(c->device);
+    join_extract(c);
     memset(vol_out, 0, sizeof(*vol_out));
     memset(out, 0, sizeof(*out));
     mtx_volume v{};
@@ -668,6 +699,7 @@ mtx_status mtx_upload_compute_min_max_mip(mtx_context_t c, const void *host, con
 mtx_status mtx_minmax_free(mtx_context_t c, mtx_minmax_output *mm) {
     if (!c || !mm) return MTX_ERR_INVALID_ARG;
     DeviceGuard g(c->device);
+    join_extract(c);
     dev_free(c, mm->minMaxImage.ptr);
     memset(mm, 0, sizeof(*mm));
     return MTX_OK;
@@ -681,6 +713,7 @@ mtx_status mtx_filter_active_blocks(mtx_context_t c, const mtx_minmax_output *mm
     mtx_status r = check_pc(c, &mm->volumeImage, pc);
     if (r != MTX_OK) return r;
     DeviceGuard g(c->device);
+    join_extract(c);
     memset(out, 0, sizeof(*out));
     const Problem p = make_problem(&mm->volumeImage, pc->blockDim[0], pc->isovalue);
     void *ids = nullptr, *cnt = nullptr, *rank = nullptr;
@@ -712,6 +745,7 @@ mtx_status mtx_filter_active_blocks(mtx_context_t c, const mtx_minmax_output *mm
 mtx_status mtx_read_active_block_count(mtx_context_t c, mtx_filtering_output *f) {
     if (!c || !f || !f->activeBlockCountBuffer.ptr) return MTX_ERR_INVALID_ARG;
     DeviceGuard g(c->device);
+    join_extract(c);
     MTX_CUDA(c, cudaMemcpyAsync(c->pinned, f->activeBlockCountBuffer.ptr, 4, cudaMemcpyDeviceToHost, c->stream));
     MTX_CUDA(c, cudaStreamSynchronize(c->stream));
     mtx_status r = check_device_status(c);
@@ -725,6 +759,7 @@ mtx_status mtx_read_buffer(mtx_context_t c, const mtx_buffer *src, uint64_t offs
     if (offset > src->size || bytes > src->size - offset) return fail(c, MTX_ERR_INVALID_ARG, "read past the buffer");
     if (!bytes) return MTX_OK;
     DeviceGuard g(c->device);
+    join_extract(c);
     MTX_CUDA(c, cudaMemcpyAsync(host, (const char *)src->ptr + offset, bytes, cudaMemcpyDeviceToHost, c->stream));
     MTX_CUDA(c, cudaStreamSynchronize(c->stream));
     return MTX_OK;
@@ -733,6 +768,7 @@ mtx_status mtx_read_buffer(mtx_context_t c, const mtx_buffer *src, uint64_t offs
 mtx_status mtx_filtering_free(mtx_context_t c, mtx_filtering_output *f) {
     if (!c || !f) return MTX_ERR_INVALID_ARG;
     DeviceGuard g(c->device);
+    join_extract(c);
     dev_free(c, f->compactedBlockIdBuffer.ptr);
     dev_free(c, f->activeBlockCountBuffer.ptr);
     dev_free(c, f->blockRankBuffer.ptr);
@@ -757,6 +793,7 @@ mtx_status mtx_extract_meshlet_descriptors(mtx_context_t c, const mtx_minmax_out
     mtx_status r = check_pc(c, &mm->volumeImage, pc);
     if (r != MTX_OK) return r;
     DeviceGuard g(c->device);
+    join_extract(c);
     memset(out, 0, sizeof(*out));
     const mtx_extract_options o = default_opts(opts_in);
     if (o.vertexFormat > MTX_VERTEX_DATA || o.frame > MTX_FRAME_NDC || o.staging > MTX_STAGING_LDG)
@@ -844,6 +881,7 @@ mtx_status mtx_extract_meshlet_descriptors(mtx_context_t c, const mtx_minmax_out
 mtx_status mtx_extraction_free(mtx_context_t c, mtx_extraction_output *x) {
     if (!c || !x) return MTX_ERR_INVALID_ARG;
     DeviceGuard g(c->device);
+    join_extract(c);
     dev_free(c, x->vertexBuffer.ptr);
     dev_free(c, x->indexBuffer.ptr);
     dev_free(c, x->meshletDescriptorBuffer.ptr);
@@ -903,11 +941,19 @@ mtx_status mtx_extract_plain_async(mtx_context_t c, const mtx_volume *vol, const
         prof_end(P, s);
         if (r != MTX_OK) return r;
     }
+    // the filter overwrites the ids, ranks and count a previous call's extraction may still read
+    if ((r = join_extract(c)) != MTX_OK) return r;
     prof_begin(P, "Active_Block_Filtering", s);
     r = launch_filter(c, p, (const uint2 *)c->leaf.ptr, (uint32_t *)c->ids.ptr, (uint32_t *)c->rank.ptr,
                       &c->ctrl->active_count, nullptr, s);
     prof_end(P, s);
     if (r != MTX_OK) return r;
+    cudaStream_t es = s;  // the extraction passes' stream
+    if (c->has_xstream) {
+        es = c->xstream;
+        MTX_CUDA(c, cudaEventRecord(c->ev_filtered, s));
+        MTX_CUDA(c, cudaStreamWaitEvent(es, c->ev_filtered, 0));
+    }
     ExtractArgs a;
     memset(&a, 0, sizeof(a));
     a.ids = (const uint32_t *)c->ids.ptr;
@@ -931,20 +977,24 @@ mtx_status mtx_extract_plain_async(mtx_context_t c, const mtx_volume *vol, const
     a.normals = o.normals;
     a.staging = o.staging;
     a.threads = o.threads;
-    prof_begin(P, "Mesh_Extraction_Count", s);
-    r = launch_count(c, p, a, s);
-    prof_end(P, s);
+    prof_begin(P, "Mesh_Extraction_Count", es);
+    r = launch_count(c, p, a, es);
+    prof_end(P, es);
     if (r != MTX_OK) return r;
-    prof_begin(P, "Mesh_Extraction_Emit", s);
-    r = launch_emit(c, p, a, s);
-    prof_end(P, s);
+    prof_begin(P, "Mesh_Extraction_Emit", es);
+    r = launch_emit(c, p, a, es);
+    prof_end(P, es);
     if (r != MTX_OK) return r;
     if (desc != out->meshlets && out->meshlets && out->meshletCapacity) {
         // the caller's descriptor buffer was too small for the bound: copy what fits
         MTX_CUDA(c, cudaMemcpyAsync(out->meshlets, desc, out->meshletCapacity * sizeof(mtx_meshlet_descriptor),
-                                    cudaMemcpyDeviceToDevice, s));
+                                    cudaMemcpyDeviceToDevice, es));
     }
-    MTX_CUDA(c, cudaMemcpyAsync(out->counters + 4, &c->ctrl->status.code, 4, cudaMemcpyDeviceToDevice, s));
+    MTX_CUDA(c, cudaMemcpyAsync(out->counters + 4, &c->ctrl->status.code, 4, cudaMemcpyDeviceToDevice, es));
+    if (c->has_xstream) {
+        MTX_CUDA(c, cudaEventRecord(c->ev_extracted, es));
+        c->extract_pending = true;
+    }
     return MTX_OK;
 }
 

@@ -112,6 +112,7 @@ extern "C" mtx_status mtx_autotune(mtx_context_t c, const mtx_volume *vol, float
                                    uint32_t flags, mtx_autotune_result *out) {
     if (!c || !vol || !out) return c ? fail(c, MTX_ERR_INVALID_ARG, "null argument") : MTX_ERR_INVALID_ARG;
     DeviceGuard dg(c->device);
+    join_extract(c);
     mtx_status rs = check_volume(c, vol);
     if (rs != MTX_OK) return rs;
     memset(out, 0, sizeof(*out));

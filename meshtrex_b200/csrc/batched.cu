@@ -674,6 +674,7 @@ mtx_status mtx_batch_create(mtx_context_t c, const mtx_batch_desc *d, mtx_batch_
     if (!c || !d || !out) return MTX_ERR_INVALID_ARG;
     *out = nullptr;
     DeviceGuard dg(c->device);
+    join_extract(c);
     if (d->volumeCount == 0 || d->jobCount == 0 || !d->volumes || !d->blockEdges || !d->jobs)
         return fail(c, MTX_ERR_INVALID_ARG, "batch: empty volume or job list");
     if (d->vertexFormat > MTX_VERTEX_DATA || d->frame > MTX_FRAME_NDC)
@@ -859,6 +860,7 @@ mtx_status mtx_batch_run(mtx_batch_t b) {
     if (!b) return MTX_ERR_INVALID_ARG;
     mtx_context *c = b->ctx;
     DeviceGuard dg(c->device);
+    join_extract(c);
     if (!b->use_graph) return batch_enqueue(b, c->stream);
     if (!b->exec) {
         if (!b->capture_stream) MTX_CUDA(c, cudaStreamCreateWithFlags(&b->capture_stream, cudaStreamNonBlocking));
@@ -893,6 +895,7 @@ mtx_status mtx_batch_read_results(mtx_batch_t b, mtx_batch_job_result *results, 
     if (!b) return MTX_ERR_INVALID_ARG;
     mtx_context *c = b->ctx;
     DeviceGuard dg(c->device);
+    join_extract(c);
     MTX_CUDA(c, cudaStreamSynchronize(c->stream));
     if (results)
         MTX_CUDA(c, cudaMemcpy(results, b->args.res, sizeof(mtx_batch_job_result) * b->njobs, cudaMemcpyDeviceToHost));
@@ -914,6 +917,7 @@ mtx_status mtx_batch_read_results(mtx_batch_t b, mtx_batch_job_result *results, 
 mtx_status mtx_batch_destroy(mtx_batch_t b) {
     if (!b) return MTX_ERR_INVALID_ARG;
     DeviceGuard dg(b->ctx->device);
+    join_extract(b->ctx);
     batch_release(b);
     return MTX_OK;
 }

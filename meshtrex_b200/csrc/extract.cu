@@ -209,6 +209,7 @@ static mtx_status grid_for(mtx_context *c, K kernel, int threads, uint32_t smem,
     int per_sm = 0;
     MTX_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem));
     if (per_sm < 1) return fail(c, MTX_ERR_UNSUPPORTED, "extraction kernel does not fit on an SM");
+    if (c->tuning.extractCtasPerSm) per_sm = std::min(per_sm, (int)c->tuning.extractCtasPerSm);
     uint64_t g = (uint64_t)per_sm * c->sm_count;
     if (host_count) g = std::min<uint64_t>(g, (host_count + warps - 1) / warps);
     grid = (unsigned)std::max<uint64_t>(g, 1);

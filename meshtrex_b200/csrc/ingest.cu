@@ -53,6 +53,7 @@ mtx_status mtx_parse_volume_name(const char *path, uint32_t dims[3], uint32_t *d
 mtx_status mtx_volume_load(mtx_context_t c, const char *path, mtx_volume *out) {
     if (!c || !path || !out) return c ? fail(c, MTX_ERR_INVALID_ARG, "null argument") : MTX_ERR_INVALID_ARG;
     DeviceGuard dg(c->device);
+    join_extract(c);
     memset(out, 0, sizeof(*out));
     uint32_t dims[3], dtype;
     mtx_status rs = mtx_parse_volume_name(path, dims, &dtype);

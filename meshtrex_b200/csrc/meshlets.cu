@@ -113,6 +113,7 @@ extern "C" mtx_status mtx_build_meshlets(mtx_context_t c, const mtx_extraction_o
                                          uint32_t maxPrimitives, mtx_meshlet_output *out) {
     if (!c) return MTX_ERR_INVALID_ARG;
     DeviceGuard dg(c->device);
+    join_extract(c);
     if (!ext || !out) return fail(c, MTX_ERR_INVALID_ARG, "null argument");
     memset(out, 0, sizeof(*out));
     if (maxVertices < 3 || maxVertices > kMaxMeshletVertices || maxPrimitives < 1 || maxPrimitives > 1024)
@@ -182,6 +183,7 @@ extern "C" mtx_status mtx_build_meshlets(mtx_context_t c, const mtx_extraction_o
 extern "C" mtx_status mtx_meshlet_output_free(mtx_context_t c, mtx_meshlet_output *out) {
     if (!c || !out) return MTX_ERR_INVALID_ARG;
     DeviceGuard dg(c->device);
+    join_extract(c);
     dev_free(c, out->meshletDescriptorBuffer.ptr);
     dev_free(c, out->meshletVertexBuffer.ptr);
     dev_free(c, out->vertexBuffer.ptr);

@@ -47,8 +47,14 @@ struct mtx_context {
     mtx::Scratch filter_status, count_status, faces, state, leaf, ids, rank, desc, misc;
     mtx::Scratch adj_partial, adj_iso;  // adjoint: per-block partial tiles and isovalue sums
     mtx_profiler *prof = nullptr;  // records stage times of calls given no profiler
-    mtx_tuning tuning = {0, 0, 0, 0};
+    mtx_tuning tuning = {0, 0, 0, 0, 0};
     cudaStream_t copy_stream = nullptr;  // host-to-device slabs of mtx_upload_compute_min_max_mip (made on first use)
+    // mtx_context_set_extract_stream: count/scan/emit of the async call on a second stream
+    bool has_xstream = false;
+    cudaStream_t xstream = nullptr;
+    cudaEvent_t ev_filtered = nullptr;   // filter done on `stream` (the extraction may start)
+    cudaEvent_t ev_extracted = nullptr;  // extraction done on `xstream` (the scratch is free again)
+    bool extract_pending = false;        // ev_extracted recorded and not yet joined into `stream`
 };
 
 namespace mtx {
@@ -77,6 +83,10 @@ mtx_status cuda_fail(mtx_context *c, cudaError_t e, const char *what);
 mtx_status dev_alloc(mtx_context *c, void **p, size_t bytes);
 void dev_free(mtx_context *c, void *p);  // ordered on c's stream (c may be null: a device-wide wait)
 mtx_status scratch_reserve(mtx_context *c, Scratch &s, size_t bytes);
+// Makes the context's stream wait for an extraction still running on its
+// extraction stream (mtx_context_set_extract_stream); every entry point that
+// queues work on the context or touches its scratch calls it first.
+mtx_status join_extract(mtx_context *c);
 
 inline uint32_t dtype_size(uint32_t dt) { return dt == MTX_DTYPE_U8 ? 1u : dt == MTX_DTYPE_U16 ? 2u : 4u; }
 inline uint64_t nvox(const uint32_t d[3]) { return (uint64_t)d[0] * d[1] * d[2]; }

@@ -63,4 +63,5 @@ def test_autotune_reads_a_cache_file_written_before(ctx, tmp_path):
     cache.write_text(f"28 24 20 2 16 0 4 8 2 1.250000 {name}\n28 24 20 1 4 0 1 2 1 9.0 {name}\n")
     r = api.autotune(ctx, vol, 0.0, cache_path=str(cache))
     assert r["fromCache"] == 1 and r["blockEdge"] == 16 and r["ms"] == 1.25
-    assert r["tuning"] == {"minmaxZChunk": 0, "minmaxSlices": 4, "extractWarps": 8, "staging": 2}
+    assert r["tuning"] == {"minmaxZChunk": 0, "minmaxSlices": 4, "extractWarps": 8, "staging": 2,
+                           "extractCtasPerSm": 0}

@@ -221,3 +221,46 @@ def test_invalid_arguments_are_rejected(ctx):
     with pytest.raises(L.MtxError) as e:
         api.compute_min_max_mip(ctx, v, pc)
     assert e.value.status == 2
+
+
+def test_extraction_stream_overlaps_and_matches_oracle(oracle):
+    """With an extraction stream (mtx_context_set_extract_stream), the whole-path
+    call queues count, scan and emit there; back-to-back calls on the same
+    context reuse its scratch only after the previous extraction, and a drop-in
+    call afterwards joins it.  Every output must still be the oracle's, with the
+    count and emit passes capped to two CTAs an SM."""
+    from meshtrex_b200 import api
+    a = blob_volume((48, 40, 64), np.uint16, seed=41)
+    b = blob_volume((40, 48, 32), np.uint8, seed=42)
+    isos_a = [mid_iso(a), float(np.percentile(a, 30))]
+    refs = [oracle.extract(a, 8, iso) for iso in isos_a]
+    va, vb = to_cuda(a), to_cuda(b)
+    ls, xs = torch.cuda.Stream(), torch.cuda.Stream()
+    c = api.Context(0, stream=ls)
+    try:
+        c.set_extract_stream(xs)
+        c.set_tuning(extract_ctas_per_sm=2)
+        exts = [api.AsyncExtractor(c, va, 8, iso, r.n_vertices + 5, r.n_triangles + 5) for iso, r in zip(isos_a, refs)]
+        for _ in range(3):
+            for e in exts:
+                e.run()
+        c.synchronize()
+        for e, r in zip(exts, refs):
+            cnt = u32(e.counters)
+            assert cnt[4] == 0 and cnt[0] == r.n_vertices and cnt[1] == 3 * r.n_triangles
+            np.testing.assert_array_equal(e.vertices[: r.n_vertices].cpu().numpy().view(np.uint32),
+                                          r.xyz.view(np.uint32))
+            np.testing.assert_array_equal(u32(e.indices[: r.n_triangles]), r.indices)
+        # a drop-in call on the same context after an asynchronous one
+        exts[0].run()
+        iso_b = mid_iso(b)
+        m = api.extract(vb, 4, iso_b, ctx=c)
+        rb = oracle.extract(b, 4, iso_b)
+        np.testing.assert_array_equal(m.vertices.cpu().numpy().view(np.uint32), rb.xyz.view(np.uint32))
+        np.testing.assert_array_equal(u32(m.indices), rb.indices)
+        c.set_extract_stream(None)
+        exts[1].run()
+        c.synchronize()
+        assert u32(exts[1].counters)[0] == refs[1].n_vertices
+    finally:
+        c.close()
