@@ -216,6 +216,16 @@ mtx_status mtx_synchronize(mtx_context_t ctx);
 /* Host-side fault injection for tests: the k-th device allocation from now
  * fails with MTX_ERR_OOM (k = 0 disables). */
 mtx_status mtx_debug_fail_allocation(mtx_context_t ctx, uint32_t k);
+/* Failure injection for tests of the bounded waits, on the host: the
+ * look-back waits of this context's compaction and count scans give up after
+ * max_polls polls (0: the built-in bound of about a second), and withhold
+ * bit 0 (compaction) / bit 1 (count scan) makes the next launches skip the
+ * ticket of their first tile, so that every later tile waits for a
+ * predecessor that never publishes.  Those tiles give up, record
+ * MTX_ERR_TIMEOUT (reported by mtx_synchronize) and abort their successors;
+ * the context stays usable.  mtx_debug_set_waits(ctx, 0, 0) restores normal
+ * operation.  No meshtrex counterpart. */
+mtx_status mtx_debug_set_waits(mtx_context_t ctx, uint32_t max_polls, uint32_t withhold);
 
 /* ------------------------------------------------------------- volume */
 

@@ -10,7 +10,9 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libmeshtrex_b200.so")
+# MESHTREX_B200_LIB selects another build of the library, such as the
+# bounds-check build libmeshtrex_b200_check.so (`make -C meshtrex_b200/csrc check`).
+LIB_PATH = os.environ.get("MESHTREX_B200_LIB") or os.path.join(HERE, "libmeshtrex_b200.so")
 
 MTX_OK = 0
 STATUS = {0: "MTX_OK", 1: "MTX_ERR_INVALID_ARG", 2: "MTX_ERR_UNSUPPORTED", 3: "MTX_ERR_OOM",
@@ -150,6 +152,7 @@ SIGNATURES = [
     ("mtx_context_last_error", C.c_char_p, [_P]),
     ("mtx_synchronize", _ST, [_P]),
     ("mtx_debug_fail_allocation", _ST, [_P, C.c_uint32]),
+    ("mtx_debug_set_waits", _ST, [_P, C.c_uint32, C.c_uint32]),
     ("mtx_volume_upload", _ST, [_P, _P, C.POINTER(C.c_uint32), C.c_uint32, C.POINTER(Volume)]),
     ("mtx_volume_wrap", _ST, [_P, C.POINTER(C.c_uint32), C.c_uint32, C.POINTER(Volume)]),
     ("mtx_volume_free", _ST, [_P, C.POINTER(Volume)]),

@@ -97,6 +97,10 @@ class Context:
         L.check(L.lib().mtx_context_get_tuning(self.handle, C.byref(t)), "mtx_context_get_tuning")
         return {f: getattr(t, f) for f, _ in L.Tuning._fields_}
 
+    def set_waits(self, max_polls: int = 0, withhold: int = 0):
+        """Failure injection of the bounded waits (mtx_debug_set_waits)."""
+        L.check(L.lib().mtx_debug_set_waits(self.handle, max_polls, withhold), "mtx_debug_set_waits")
+
     def fail_allocation(self, k: int):
         L.check(L.lib().mtx_debug_fail_allocation(self.handle, k), "mtx_debug_fail_allocation")
 

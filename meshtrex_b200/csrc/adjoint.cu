@@ -182,6 +182,8 @@ __global__ void __launch_bounds__(kIsoThreads) adjoint_iso_kernel(const float *_
     if (threadIdx.x == 0) *out = (float)s[0];
 }
 
+MTX_BC_READER(bc_take_adjoint)
+
 }  // namespace mtx
 
 using namespace mtx;

@@ -368,7 +368,25 @@ Problem make_problem(const mtx_volume *v, uint32_t B, float iso) {
     return p;
 }
 
+#ifdef MTX_BOUNDS_CHECK
+DevStatus bc_take_extract();
+DevStatus bc_take_filter();
+DevStatus bc_take_minmax();
+DevStatus bc_take_batched();
+DevStatus bc_take_adjoint();
+#endif
+
 static mtx_status check_device_status(mtx_context *c) {
+#ifdef MTX_BOUNDS_CHECK
+    // a bounds-check build: the translation units' check records first
+    for (DevStatus b : {bc_take_extract(), bc_take_filter(), bc_take_minmax(), bc_take_batched(), bc_take_adjoint()})
+        if (b.code) {
+            char buf[160];
+            snprintf(buf, sizeof(buf), "bounds check failed at site %u: index %u, bound %u", b.where, b.info0,
+                     b.info1);
+            return fail(c, MTX_ERR_INTERNAL, buf);
+        }
+#endif
     DevStatus h;
     MTX_CUDA(c, cudaMemcpy(&h, &c->ctrl->status, sizeof(h), cudaMemcpyDeviceToHost));
     if (h.code == 0) return MTX_OK;
@@ -478,6 +496,13 @@ mtx_status mtx_synchronize(mtx_context_t c) {
 mtx_status mtx_debug_fail_allocation(mtx_context_t c, uint32_t k) {
     if (!c) return MTX_ERR_INVALID_ARG;
     c->fail_alloc_in = k;
+    return MTX_OK;
+}
+
+mtx_status mtx_debug_set_waits(mtx_context_t c, uint32_t max_polls, uint32_t withhold) {
+    if (!c || withhold > 3u) return MTX_ERR_INVALID_ARG;
+    c->wait_polls = max_polls;
+    c->withhold = withhold;
     return MTX_OK;
 }
 

@@ -583,6 +583,8 @@ __global__ void __launch_bounds__(kBThreads) batch_extract_kernel(const __grid_c
     }
 }
 
+MTX_BC_READER(bc_take_batched)
+
 }  // namespace mtx
 
 // ------------------------------------------------------------------ host

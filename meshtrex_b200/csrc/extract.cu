@@ -89,7 +89,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32)
 // -------------------------------------------------------------- scan pass
 __global__ void __launch_bounds__(kScanThreads)
     pmb_scan_kernel(mtx_meshlet_descriptor *__restrict__ desc, const uint32_t *__restrict__ count_ptr,
-                    uint64_t *tile_status, uint32_t *ticket, uint32_t *totals, DevStatus *st) {
+                    uint64_t *tile_status, uint32_t *ticket, uint32_t *totals, DevStatus *st, uint32_t spin_limit) {
     __shared__ uint32_t s_tile, s_ok;
     __shared__ uint64_t s_tmp[kScanThreads / 32 + 1];
     __shared__ uint64_t s_pre[2];
@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(kScanThreads)
     const uint32_t t = s_tile;
     const uint32_t count = *count_ptr;
     if (t >= (count + kScanTile - 1) / kScanTile) return;
-    scan_tile(desc, count, t, tile_status, totals, st, s_tmp, &s_ok, s_pre);
+    scan_tile(desc, count, t, tile_status, totals, st, s_tmp, &s_ok, s_pre, spin_limit);
 }
 
 // -------------------------------------------------------------- emit pass
@@ -170,9 +170,10 @@ __global__ void __launch_bounds__(kMaxWarps * 32, (!GENERIC && CPL == 8) ? 3 : 1
             dn = desc[rn];
             nb_rk_n = neighbour_rank(p, gn, idn, rank_map);
         }
-        const uint32_t nb_vb = (nb_rk != kNoVertex) ? __ldg(&desc[nb_rk].vertexOffset) : kNoVertex;
+        const uint32_t nb_vb =
+            (nb_rk != kNoVertex && MTX_BC(nb_rk, count, kBcDesc)) ? __ldg(&desc[nb_rk].vertexOffset) : kNoVertex;
         uint32_t rec[CPL];
-        gather_issue_map<CPL>(p, pl, g, nb_rk, faces, 3 * pl.BB, cmap, rec);
+        gather_issue_map<CPL>(p, pl, g, nb_rk, faces, 3 * pl.BB, cmap, rec, block_cap * 3 * pl.BB);
         if (!tile_wait<T, TMA>(p, pl, ws, buf, g, parity, st)) {
             if (have_next && pl.nbuf == 2) tile_drain<TMA>(pl, ws, buf ^ 1u, parity);
             break;
@@ -300,8 +301,13 @@ mtx_status launch_count(mtx_context *c, const Problem &p, const ExtractArgs &a, 
     MTX_CUDA(c, cudaMemsetAsync(a.totals, 0, 4 * sizeof(uint32_t), s));
     MTX_CUDA(c, cudaMemsetAsync(c->count_status.ptr, 0, sizeof(uint64_t) * ntiles, s));
     if ((r = launch_stage<false>(c, p, a, s)) != MTX_OK) return r;
+    if (c->withhold & 2u) {  // failure injection: scan tile 0 is never handed out
+        static const uint32_t kOne = 1;
+        MTX_CUDA(c, cudaMemcpyAsync(&c->ctrl->count_ticket, &kOne, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    }
     pmb_scan_kernel<<<ntiles, kScanThreads, 0, s>>>(a.desc, a.count, (uint64_t *)c->count_status.ptr,
-                                                    &c->ctrl->count_ticket, a.totals, &c->ctrl->status);
+                                                    &c->ctrl->count_ticket, a.totals, &c->ctrl->status,
+                                                    c->wait_polls ? c->wait_polls : kSpinLimit);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "scan launch");
     return MTX_OK;
@@ -318,7 +324,8 @@ mtx_status launch_desc_scan(mtx_context *c, mtx_meshlet_descriptor *desc, const 
     MTX_CUDA(c, cudaMemsetAsync(totals, 0, 4 * sizeof(uint32_t), s));
     MTX_CUDA(c, cudaMemsetAsync(c->count_status.ptr, 0, sizeof(uint64_t) * ntiles, s));
     pmb_scan_kernel<<<ntiles, kScanThreads, 0, s>>>(desc, count, (uint64_t *)c->count_status.ptr,
-                                                    &c->ctrl->count_ticket, totals, &c->ctrl->status);
+                                                    &c->ctrl->count_ticket, totals, &c->ctrl->status,
+                                                    c->wait_polls ? c->wait_polls : kSpinLimit);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "scan launch");
     return MTX_OK;
@@ -328,5 +335,7 @@ mtx_status launch_desc_scan(mtx_context *c, mtx_meshlet_descriptor *desc, const 
 mtx_status launch_emit(mtx_context *c, const Problem &p, const ExtractArgs &a, cudaStream_t s) {
     return launch_stage<true>(c, p, a, s);
 }
+
+MTX_BC_READER(bc_take_extract)
 
 }  // namespace mtx

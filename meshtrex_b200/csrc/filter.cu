@@ -33,7 +33,7 @@ __global__ void __launch_bounds__(kFilterThreads)
     filter_compact_kernel(const uint2 *__restrict__ leaf, uint64_t nblocks, uint32_t ntiles, uint32_t dtype,
                           float iso, uint32_t *__restrict__ ids, uint32_t *__restrict__ rank_map,
                           uint32_t *__restrict__ count_out, uint64_t *__restrict__ count_status,
-                          uint32_t *tile_status, uint32_t *ticket, DevStatus *st) {
+                          uint32_t *tile_status, uint32_t *ticket, DevStatus *st, uint32_t spin_limit) {
     __shared__ uint32_t s_tile, s_prefix, s_abort;
     __shared__ uint32_t s_tmp[kFilterThreads / 32 + 1];
     if (threadIdx.x == 0) {
@@ -92,7 +92,7 @@ __global__ void __launch_bounds__(kFilterThreads)
                 const uint32_t first = inc ? (uint32_t)(__ffs(inc) - 1) : 32u;
                 const uint32_t window = first >= 31 ? 0xffffffffu : ((2u << first) - 1u);
                 if (emp & window) {
-                    if (++spins >= kSpinLimit) {
+                    if (++spins >= spin_limit) {
                         if (lane == 0) report(st, MTX_ERR_TIMEOUT, kSiteFilterLookback, t, (uint32_t)j);
                         abort = true;
                         break;
@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(kFilterThreads)
 #pragma unroll
     for (int i = 0; i < ITEMS; ++i) {
         rk[i] = 0xffffffffu;
-        if (f[i]) {
+        if (f[i] && MTX_BC(r, nblocks, kBcRank)) {
             const uint32_t id = (uint32_t)(base + i);
             ids[r] = id;
             rk[i] = r;
@@ -144,6 +144,8 @@ __global__ void __launch_bounds__(kFilterThreads)
     if (t == ntiles - 1 && threadIdx.x == 0) *count_out = s_prefix + total;
 }
 
+MTX_BC_READER(bc_take_filter)
+
 mtx_status launch_filter(mtx_context *c, const Problem &p, const uint2 *leaf, uint32_t *ids, uint32_t *rank_map,
                          uint32_t *count, uint64_t *count_status, cudaStream_t s) {
     if (p.nblocks >= (1ull << 30)) return fail(c, MTX_ERR_UNSUPPORTED, "more than 2^30 blocks");
@@ -158,9 +160,14 @@ mtx_status launch_filter(mtx_context *c, const Problem &p, const uint2 *leaf, ui
         MTX_CUDA(c, cudaMemsetAsync(&c->ctrl->filter_ticket, 0, sizeof(uint32_t), s));
         MTX_CUDA(c, cudaMemsetAsync(count, 0, sizeof(uint32_t), s));
     }
+    if (c->withhold & 1u) {  // failure injection: tile 0 is never handed out, so its successors wait and give up
+        static const uint32_t kOne = 1;
+        MTX_CUDA(c, cudaMemcpyAsync(&c->ctrl->filter_ticket, &kOne, sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    }
     filter_compact_kernel<kFilterItems><<<ntiles, kFilterThreads, 0, s>>>(
         leaf, p.nblocks, ntiles, p.dtype, p.iso, ids, rank_map, count, count_status,
-        (uint32_t *)c->filter_status.ptr, &c->ctrl->filter_ticket, &c->ctrl->status);
+        (uint32_t *)c->filter_status.ptr, &c->ctrl->filter_ticket, &c->ctrl->status,
+        c->wait_polls ? c->wait_polls : kSpinLimit);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "filter launch");
     return MTX_OK;
@@ -284,7 +291,7 @@ extern "C" mtx_status mtx_filter_active_blocks_noalloc(const uint32_t *leaf_minm
     }
     filter_compact_kernel<kNoallocItems><<<ntiles, kFilterThreads, 0, s>>>(
         reinterpret_cast<const uint2 *>(leaf_minmax), total_blocks, ntiles, dtype, isovalue, compacted_ids, block_rank,
-        active_count, nullptr, sc, sc + kNoallocTicket, st);
+        active_count, nullptr, sc, sc + kNoallocTicket, st, kSpinLimit);
     if (cudaGetLastError() != cudaSuccess) return MTX_ERR_CUDA;
     return MTX_OK;
 }

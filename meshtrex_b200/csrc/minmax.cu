@@ -253,7 +253,8 @@ __global__ void __launch_bounds__(128) minmax_leaf_tma_kernel(const __grid_const
                         lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
                         hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
                     }
-                    if (row_on && on && (lane % LPB) == 0)
+                    if (row_on && on && (lane % LPB) == 0 &&
+                        MTX_BC(((uint64_t)bz * a.GY + by) * a.GX + x0 / B + j, (uint64_t)a.GX * a.GY * a.GZ, kBcLeaf))
                         leaf[((uint64_t)bz * a.GY + by) * a.GX + x0 / B + j] = make_uint2(lo, hi);
                     amn[j] = smn[j];
                     amx[j] = smx[j];
@@ -282,7 +283,8 @@ __global__ void __launch_bounds__(128) minmax_leaf_tma_kernel(const __grid_const
                     lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
                     hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
                 }
-                if (row_on && on && (lane % LPB) == 0)
+                if (row_on && on && (lane % LPB) == 0 &&
+                    MTX_BC(((uint64_t)bz * a.GY + by) * a.GX + x0 / B + j, (uint64_t)a.GX * a.GY * a.GZ, kBcLeaf))
                     leaf[((uint64_t)bz * a.GY + by) * a.GX + x0 / B + j] = make_uint2(lo, hi);
                 clo = lo;
                 chi = hi;
@@ -539,5 +541,7 @@ mtx_status launch_pyramid(mtx_context *c, uint2 *all, int levels, const uint32_t
     if (e != cudaSuccess) return cuda_fail(c, e, "pyramid launch");
     return MTX_OK;
 }
+
+MTX_BC_READER(bc_take_minmax)
 
 }  // namespace mtx

@@ -203,7 +203,8 @@ __device__ __forceinline__ void minmax_leaf_vec_warp(const T *__restrict__ vol, 
                     }
                     if (on && (lane % LPB) == 0) {
                         const uint32_t bx = x0 / B + j;
-                        leaf[((uint64_t)bz * GY + by) * GX + bx] = make_uint2(a, b);
+                        if (MTX_BC(((uint64_t)bz * GY + by) * GX + bx, (uint64_t)GX * GY * GZ, kBcLeaf))
+                            leaf[((uint64_t)bz * GY + by) * GX + bx] = make_uint2(a, b);
                     }
                     amn[j] = smn[j];
                     amx[j] = smx[j];
@@ -223,7 +224,8 @@ __device__ __forceinline__ void minmax_leaf_vec_warp(const T *__restrict__ vol, 
             }
             if (on && (lane % LPB) == 0) {
                 const uint32_t bx = x0 / B + j;
-                leaf[((uint64_t)bz * GY + by) * GX + bx] = make_uint2(a, b);
+                if (MTX_BC(((uint64_t)bz * GY + by) * GX + bx, (uint64_t)GX * GY * GZ, kBcLeaf))
+                    leaf[((uint64_t)bz * GY + by) * GX + bx] = make_uint2(a, b);
             }
         }
     }

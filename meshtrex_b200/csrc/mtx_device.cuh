@@ -41,6 +41,55 @@ __device__ __forceinline__ void report(DevStatus *st, uint32_t code, uint32_t wh
     }
 }
 
+// ----------------------------------------------------------- bounds checks
+// A debug build of the library (-DMTX_BOUNDS_CHECK, `make check`) checks the
+// shared- and global-memory indices of the extraction kernels: an index
+// outside its range is recorded in the translation unit's check record
+// (site, index, bound), the access is skipped, and mtx_synchronize reports
+// the record as MTX_ERR_INTERNAL.  There is no trap.  In the normal build
+// MTX_BC is the constant true and the checks compile away.
+enum : uint32_t {
+    kBcTile = 101,      // voxel tile in shared memory
+    kBcRows = 102,      // inside masks, crossing rows, prefixes, case bytes, mixed masks
+    kBcJobs = 103,      // job window
+    kBcVertex = 104,    // vertex buffer
+    kBcIndex = 105,     // index buffer
+    kBcFaces = 106,     // face records (read and write)
+    kBcContext = 107,   // context layer (neighbour ids and masks)
+    kBcVoxTab = 108,    // voxel table
+    kBcState = 109,     // block state
+    kBcRank = 110,      // rank map and compacted ids
+    kBcLeaf = 111,      // min/max leaf level
+    kBcDesc = 112,      // meshlet descriptors
+};
+#ifdef MTX_BOUNDS_CHECK
+static __device__ DevStatus g_bc_record;
+__device__ __forceinline__ bool bc_ok(uint64_t i, uint64_t n, uint32_t site) {
+    if (i < n) return true;
+    if (atomicCAS(&g_bc_record.code, 0u, (uint32_t)MTX_ERR_INTERNAL) == 0u) {
+        g_bc_record.where = site;
+        g_bc_record.info0 = (uint32_t)i;
+        g_bc_record.info1 = (uint32_t)n;
+    }
+    return false;
+}
+#define MTX_BC(i, n, site) ::mtx::bc_ok((uint64_t)(i), (uint64_t)(n), (site))
+// Defines the host reader of this translation unit's check record: it copies
+// the record out, clears it and returns it.
+#define MTX_BC_READER(name)                                                        \
+    ::mtx::DevStatus name() {                                                      \
+        ::mtx::DevStatus h{}, z{};                                                 \
+        if (cudaMemcpyFromSymbol(&h, ::mtx::g_bc_record, sizeof(h)) != cudaSuccess) \
+            cudaGetLastError();                                                    \
+        else if (h.code)                                                           \
+            cudaMemcpyToSymbol(::mtx::g_bc_record, &z, sizeof(z));                 \
+        return h;                                                                  \
+    }
+#else
+#define MTX_BC(i, n, site) true
+#define MTX_BC_READER(name)
+#endif
+
 __device__ __forceinline__ bool failed(const DevStatus *st) {
     return st && *(volatile const uint32_t *)&st->code != 0u;
 }

@@ -42,6 +42,8 @@ struct mtx_context {
     int max_smem_optin = 0;
     std::string last_error;
     uint32_t fail_alloc_in = 0;  // fault injection: fail the k-th allocation
+    uint32_t wait_polls = 0;     // failure injection: look-back polls before giving up (0: kSpinLimit)
+    uint32_t withhold = 0;       // failure injection: bit 0 / 1 skip the first compaction / count-scan tile
     mtx::Ctrl *ctrl = nullptr;   // device
     uint32_t *pinned = nullptr;  // pinned host words for count readbacks
     mtx::Scratch filter_status, count_status, faces, state, leaf, ids, rank, desc, misc;

@@ -205,7 +205,7 @@ __device__ __forceinline__ bool tile_wait(const Problem &p, const WPlan &pl, uns
         }
 #pragma unroll
         for (uint32_t k = 0; k < kLdgBatch; ++k)
-            if (dst[k] != 0xffffffffu) tile[dst[k]] = v[k];
+            if (dst[k] != 0xffffffffu && MTX_BC(dst[k], pl.PX * pl.B1 * pl.B1, kBcTile)) tile[dst[k]] = v[k];
     }
     __syncwarp();
     return true;
@@ -235,7 +235,7 @@ __device__ __forceinline__ void tile_load_float_from(const Problem &p, const WPl
         }
 #pragma unroll
         for (uint32_t k = 0; k < kLdgBatch; ++k)
-            if (dst[k] != 0xffffffffu) tile[dst[k]] = v[k];
+            if (dst[k] != 0xffffffffu && MTX_BC(dst[k], pl.PX * pl.B1 * pl.B1, kBcTile)) tile[dst[k]] = v[k];
     }
     __syncwarp();
 }
@@ -273,7 +273,8 @@ __device__ __forceinline__ void build_rows(const Problem &p, const WPlan &pl, un
     for (uint32_t q = threadIdx.x & 31; q < pl.B1 * pl.B1; q += 32) {
         const uint32_t z = fdiv(q, pl.rB1), y = q - z * pl.B1;
         uint32_t m = 0;
-        if (g.oy + y < p.Y && g.oz + z < p.Z) {
+        if (g.oy + y < p.Y && g.oz + z < p.Z &&
+            MTX_BC((z * pl.B1 + y) * pl.PX + g.xoff + xin, pl.PX * pl.B1 * pl.B1 + 1, kBcTile)) {
             const T *r = tile + (z * pl.B1 + y) * pl.PX + g.xoff;
             if (Vox<T>::code == 2) {
                 for (uint32_t x = 0; x < xin; ++x) m |= (Vox<T>::val(r[x]) <= p.iso ? 1u : 0u) << x;
@@ -299,7 +300,7 @@ __device__ __forceinline__ void build_rows(const Problem &p, const WPlan &pl, un
                 for (uint32_t x = 0; x < xin; ++x) m |= ((uint32_t)r[x] <= thr ? 1u : 0u) << x;
             }
         }
-        rows[q] = m;
+        if (MTX_BC(q, pl.B1 * pl.B1, kBcRows)) rows[q] = m;
     }
     __syncwarp();
 }
@@ -401,6 +402,7 @@ __device__ __forceinline__ void block_counts(const Problem &p, const WPlan &pl, 
                 mm &= mm - 1u;
                 const uint32_t cfg = cell_case(rows, pl.B1, x, y, z);
                 stri += ntab[cfg];
+                if (!MTX_BC(q * B + x, B * BB, kBcRows)) continue;
                 if (cases_out) cases_out[q * B + x] = (uint8_t)cfg;
                 if (keep) ws[pl.off_case + q * B + x] = (uint8_t)cfg;
             }
@@ -505,8 +507,9 @@ static __device__ __noinline__ float3 vertex_normal_any(const Problem &p, uint32
 template <typename T>
 __device__ __forceinline__ float3 vertex_pos(const Problem &p, const WPlan &pl, const T *tile, const Geo &g, uint32_t x,
                                              uint32_t y, uint32_t z, uint32_t a, bool ndc, float *tout) {
-    const uint32_t i0 = (z * pl.B1 + y) * pl.PX + g.xoff + x;
-    const uint32_t i1 = i0 + (a == 0 ? 1u : a == 1 ? pl.PX : pl.PX * pl.B1);
+    uint32_t i0 = (z * pl.B1 + y) * pl.PX + g.xoff + x;
+    uint32_t i1 = i0 + (a == 0 ? 1u : a == 1 ? pl.PX : pl.PX * pl.B1);
+    if (!MTX_BC(i1, pl.PX * pl.B1 * pl.B1, kBcTile)) i1 = i0 = 0;
     const float t = edge_t(Vox<T>::val(tile[i0]), Vox<T>::val(tile[i1]), p.iso);
     *tout = t;
     float3 pos = make_float3((float)(g.ox + x), (float)(g.oy + y), (float)(g.oz + z));
@@ -563,7 +566,7 @@ __device__ __forceinline__ void emit_vertices(const Problem &p, const WPlan &pl,
         const uint32_t cnt = min(kJobWin, nv - w0);
         for (uint32_t b = 0; b < cnt; b += 32) {
             const uint32_t n = min(32u, cnt - b);
-            if (lane < n) {
+            if (lane < n && MTX_BC(w0 + b + lane, nv, kBcVertex)) {
                 const uint32_t job = jobs[b + lane];
                 const uint32_t i = job & 0xfffu, a = job >> 12;
                 const uint32_t q = fdiv(i, pl.rB), x = i - q * B;
@@ -636,6 +639,10 @@ __device__ __forceinline__ uint32_t edge_vertex(uint32_t x, uint32_t y, uint32_t
         m = voxel_mask(cross, BB, q, ux);
     } else {
         const uint32_t jx = ctx_index(B, ux, uy, uz);
+        if (!MTX_BC(jx, 3 * B * B + 3 * B + 1, kBcContext)) {
+            bad = true;
+            return 0;
+        }
         base = nvid[jx];
         m = nm[jx];
     }
@@ -664,7 +671,7 @@ __device__ __forceinline__ void build_vtab(const WPlan &pl, const unsigned char 
             const uint32_t x = __ffs(any) - 1;
             any &= any - 1u;
             const uint32_t m = ((xc >> x) & 1u) | (((yc >> x) & 1u) << 1) | (((zc >> x) & 1u) << 2);
-            vt[q * B + x] = (uint16_t)(run | (m << 11));
+            if (MTX_BC(q * B + x, B * BB, kBcVoxTab)) vt[q * B + x] = (uint16_t)(run | (m << 11));
             run += __popc(m);
         }
     }
@@ -685,6 +692,10 @@ __device__ __forceinline__ uint32_t edge_vertex_vt(uint32_t x, uint32_t y, uint3
         m = v >> 11;
     } else {
         const uint32_t jx = ctx_index(B, ux, uy, uz);
+        if (!MTX_BC(jx, 3 * B * B + 3 * B + 1, kBcContext)) {
+            bad = true;
+            return 0;
+        }
         base = nvid[jx];
         m = nm[jx];
     }
@@ -708,7 +719,7 @@ constexpr uint64_t kCnt31 = 0x7fffffffull;
 // including the first inclusive one, in windows of 32 read by the warp;
 // false if a predecessor aborted or the wait timed out.
 __device__ __forceinline__ bool lookback_sum31(const uint64_t *status, uint32_t r, uint64_t &ev, uint64_t &et,
-                                               DevStatus *st) {
+                                               DevStatus *st, uint32_t spin_limit = kSpinLimit) {
     const uint32_t lane = threadIdx.x & 31;
     ev = et = 0;
     int64_t j = (int64_t)r - 1;
@@ -723,7 +734,7 @@ __device__ __forceinline__ bool lookback_sum31(const uint64_t *status, uint32_t 
         const uint32_t first = inc ? (uint32_t)(__ffs(inc) - 1) : 32u;
         const uint32_t window = first >= 31 ? 0xffffffffu : ((2u << first) - 1u);
         if (emp & window) {
-            if (++spins >= kSpinLimit) {
+            if (++spins >= spin_limit) {
                 if (lane == 0) report(st, MTX_ERR_TIMEOUT, kSiteCountLookback, r, (uint32_t)j);
                 return false;
             }
@@ -745,13 +756,14 @@ __device__ __forceinline__ bool lookback_sum31(const uint64_t *status, uint32_t 
 }
 
 __device__ __forceinline__ bool lookback_counts(uint64_t *status, uint32_t r, uint32_t bnv, uint32_t bnt,
-                                                uint64_t &ev, uint64_t &et, DevStatus *st) {
+                                                uint64_t &ev, uint64_t &et, DevStatus *st,
+                                                uint32_t spin_limit = kSpinLimit) {
     const uint32_t lane = threadIdx.x & 31;
     ev = et = 0;
     bool abort = false;
     if (r > 0) {
         if (lane == 0) st_volatile(&status[r], (1ull << 62) | ((uint64_t)bnt << 31) | bnv);
-        abort = !lookback_sum31(status, r, ev, et, st);
+        abort = !lookback_sum31(status, r, ev, et, st, spin_limit);
     }
     const uint64_t iv = ev + bnv, it = et + bnt;
     if (!abort && (iv > kCnt31 || it > kCnt31 || 3ull * it > 0xffffffffull)) {
@@ -781,7 +793,8 @@ __device__ __forceinline__ uint32_t neighbour_rank(const Problem &p, const Geo &
     uint32_t rk = kNoVertex;
     if (lane >= 1 && lane < 8) {
         const uint32_t dx = lane & 1u, dy = (lane >> 1) & 1u, dz = lane >> 2;
-        if (g.bx + dx < p.GX && g.by + dy < p.GY && g.bz + dz < p.GZ)
+        if (g.bx + dx < p.GX && g.by + dy < p.GY && g.bz + dz < p.GZ &&
+            MTX_BC((uint64_t)id + dx + dy * p.GX + (uint64_t)dz * p.GX * p.GY, p.nblocks, kBcRank))
             rk = ld_in<NC>(rank_map + id + dx + dy * p.GX + dz * p.GX * p.GY);
     }
     return rk;
@@ -831,7 +844,7 @@ __device__ __forceinline__ uint32_t ctx_map_entry(const WPlan &pl, uint32_t j) {
 template <int CPL>
 __device__ __forceinline__ void gather_issue_map(const Problem &p, const WPlan &pl, const Geo &g, uint32_t nb_rk,
                                                  const uint32_t *faces, uint32_t face_stride, const uint32_t *cmap,
-                                                 uint32_t rec[CPL]) {
+                                                 uint32_t rec[CPL], uint64_t face_words = ~0ull) {
     const uint32_t lane = threadIdx.x & 31, nb3 = pl.nb3;
     // the whole context layer lies in the volume unless the block reaches a high face
     const bool inner = g.ox + pl.B < p.X && g.oy + pl.B < p.Y && g.oz + pl.B < p.Z;
@@ -847,7 +860,8 @@ __device__ __forceinline__ void gather_issue_map(const Problem &p, const WPlan &
         if (!inner)
             take = take && g.ox + ((m >> 13) & 31u) < p.X && g.oy + ((m >> 18) & 31u) < p.Y &&
                    g.oz + ((m >> 23) & 31u) < p.Z;
-        if (take) rec[k] = __ldg(faces + (uint64_t)rk * face_stride + ((m >> 3) & 1023u)) | 0x80000000u | (c << 27);
+        if (take && MTX_BC((uint64_t)rk * face_stride + ((m >> 3) & 1023u), face_words, kBcFaces))
+            rec[k] = __ldg(faces + (uint64_t)rk * face_stride + ((m >> 3) & 1023u)) | 0x80000000u | (c << 27);
     }
 }
 
@@ -889,7 +903,7 @@ __device__ __forceinline__ void write_face_records(const WPlan &pl, const unsign
         uint32_t run = vp[q];
         for (uint32_t x = 0; x < B; ++x) {
             const uint32_t m = ((xc >> x) & 1u) | (((yc >> x) & 1u) << 1) | (((zc >> x) & 1u) << 2);
-            o[x] = run | (m << 24);
+            if (MTX_BC((uint32_t)(o - fr) + x, 3 * BB, kBcFaces)) o[x] = run | (m << 24);
             run += __popc(m);
         }
     }
@@ -985,7 +999,7 @@ __device__ __forceinline__ void emit_block(const Problem &p, const WPlan &pl, un
         const uint32_t cnt = min(kJobWin, nt - w0);
         for (uint32_t b = 0; b < cnt; b += 32) {
             const uint32_t n = min(32u, cnt - b);
-            if (lane < n) {
+            if (lane < n && MTX_BC(w0 + b + lane, nt, kBcIndex)) {
                 const uint32_t job = jobs[b + lane];
                 const uint32_t i = job & 0xfffu, t = (job >> 12) & 7u;
                 const uint32_t q = fdiv(i, pl.rB), x = i - q * B;
@@ -1023,7 +1037,7 @@ constexpr int kScanTile = kScanThreads * kScanItems;
 
 __device__ __forceinline__ void scan_tile(mtx_meshlet_descriptor *desc, uint32_t count, uint32_t t, uint64_t *status,
                                           uint32_t *totals, DevStatus *st, uint64_t *s_tmp, uint32_t *s_ok,
-                                          uint64_t *s_pre) {
+                                          uint64_t *s_pre, uint32_t spin_limit = kSpinLimit) {
     const uint32_t ntiles = (count + kScanTile - 1) / kScanTile;
     const uint32_t base = t * kScanTile + threadIdx.x * kScanItems;
     uint32_t nv[kScanItems], nt[kScanItems], sv = 0, stt = 0;
@@ -1042,7 +1056,7 @@ __device__ __forceinline__ void scan_tile(mtx_meshlet_descriptor *desc, uint32_t
     const uint64_t pre = cta_exclusive_scan64<kScanThreads>(((uint64_t)stt << 32) | sv, s_tmp, &tot);
     if (threadIdx.x < 32) {
         uint64_t ev, et;
-        const bool ok = lookback_counts(status, t, (uint32_t)tot, (uint32_t)(tot >> 32), ev, et, st);
+        const bool ok = lookback_counts(status, t, (uint32_t)tot, (uint32_t)(tot >> 32), ev, et, st, spin_limit);
         if (threadIdx.x == 0) {
             *s_ok = ok;
             s_pre[0] = ev;
