@@ -462,7 +462,8 @@ def run_mtx(args):
 
     if not args.no_batch:
         del exts
-        line["batched"] = run_batched(ctx, stream, steps=max(3, min(20, steps)), scale_down=args.batch_scale)
+        line["batched"] = run_batched(ctx, stream, steps=max(3, min(20, steps)), scale_down=args.batch_scale,
+                                      fixed=args.batch_fixed)
 
     if not args.no_backward:
         line["backward"] = run_backward(ctx, stream, steps=max(3, min(20, steps)))
@@ -471,7 +472,8 @@ def run_mtx(args):
         exts = vol = None  # release the 1024^3 volume and its outputs first
         torch.cuda.synchronize()
         torch.cuda.empty_cache()
-        line["gyroid"] = run_gyroid(ctx, stream, steps=max(3, min(10, steps)), n=args.gyroid_size)
+        line["gyroid"] = run_gyroid(ctx, stream, steps=max(3, min(10, steps)), n=args.gyroid_size,
+                                    fixed=args.gyroid_fixed)
 
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -578,7 +580,7 @@ def run_e2e(ctx, vol_dev, ws, steps):
                     "step's extractions"}
 
 
-def run_batched(ctx, stream, steps, scale_down=1):
+def run_batched(ctx, stream, steps, scale_down=1, fixed=False):
     """The 64-volume mix (anisotropic edges from {64..512}, uint8/uint16/float32,
     1-16 isovalues each, seed 3): one batched run per step (a CUDA graph of the
     batched min/max and the persistent extraction kernel) against the same
@@ -590,19 +592,28 @@ def run_batched(ctx, stream, steps, scale_down=1):
     torch.cuda.synchronize()
     t_gen = time.perf_counter() - t_gen
     vols = [it.volume for it in items]
-    blocks = [BLOCK] * len(vols)
     jobs = [(v, iso) for v, it in enumerate(items) for iso in it.isovalues]
+    # block edge of every volume and the batched kernel's block warps from the batch autotuner
+    t_tune = time.perf_counter()
+    if fixed:  # profiling runs: block 8, as many block warps as fit
+        tune = {"blockEdges": [BLOCK] * len(vols), "blockWarps": 0, "candidates": 0}
+    else:
+        tune = api.autotune_batch(ctx, vols, jobs)
+    t_tune = time.perf_counter() - t_tune
+    blocks, block_warps = tune["blockEdges"], tune["blockWarps"]
     esz = {torch.uint8: 1, torch.uint16: 2, torch.float32: 4}
     vol_bytes = sum(v.numel() * esz[v.dtype] for v in vols)
     job_voxels = sum(vols[v].numel() for v, _ in jobs)
 
     # one run sized small reports the pooled sizes it needs; the timed batch is sized exactly
-    probe = api.Batch(ctx, vols, blocks, jobs, vertex_capacity=1 << 20, triangle_capacity=1 << 20)
+    probe = api.Batch(ctx, vols, blocks, jobs, vertex_capacity=1 << 20, triangle_capacity=1 << 20,
+                      block_warps=block_warps)
     probe.run()
     _, need = probe.results(check=False)
     probe.close()
     b = api.Batch(ctx, vols, blocks, jobs, max_active_blocks=need["activeBlocks"],
-                  vertex_capacity=need["vertexCount"], triangle_capacity=need["triangleCount"], use_graph=True)
+                  vertex_capacity=need["vertexCount"], triangle_capacity=need["triangleCount"], use_graph=True,
+                  block_warps=block_warps)
     for _ in range(3):
         b.run()
     res, tot = b.results()
@@ -618,7 +629,7 @@ def run_batched(ctx, stream, steps, scale_down=1):
     res, tot = b.results()
 
     # plain per-job launches on the same jobs, outputs sized from the batch's results
-    exts = [api.AsyncExtractor(ctx, vols[v], BLOCK, iso, r["vertexCount"] + 1, r["indexCount"] // 3 + 1,
+    exts = [api.AsyncExtractor(ctx, vols[v], blocks[v], iso, r["vertexCount"] + 1, r["indexCount"] // 3 + 1,
                                max_active_blocks=r["meshletCount"] + 1)
             for (v, iso), r in zip(jobs, res)]
 
@@ -673,7 +684,8 @@ def run_batched(ctx, stream, steps, scale_down=1):
     peak, peak_kind = peak_hbm()
     out = {
         "workload": "64 volumes (edges from {64,96,128,192,256,384,512} per axis, uint8/uint16/float32 Gaussian "
-                    "blobs, seed 3), 1-16 isovalues each in the 10th-90th percentile; block 8^3"
+                    "blobs, seed 3), 1-16 isovalues each in the 10th-90th percentile; block edges and block warps "
+                    "from mtx_autotune_batch"
                     + (f"; edges divided by {scale_down}" if scale_down > 1 else ""),
         "volumes": len(vols), "jobs": len(jobs), "volume_bytes": vol_bytes, "job_voxels": job_voxels,
         "active_blocks": tot["activeBlocks"], "vertices": V, "triangles": T,
@@ -689,8 +701,12 @@ def run_batched(ctx, stream, steps, scale_down=1):
                      "what": "each volume read once + 12 B per vertex + 12 B per triangle written",
                      "peak_kind": peak_kind},
         "gpu_launches_per_step": 2,
-        "plain_launches_per_step": sum(launches_per_extraction(tuple((n + BLOCK - 1) // BLOCK for n in vols[v].shape))
-                                       for v, _ in jobs),
+        "plain_launches_per_step": sum(launches_per_extraction(tuple((n + blocks[v] - 1) // blocks[v]
+                                                                     for n in vols[v].shape)) for v, _ in jobs),
+        "autotuned": {"block_edges": sorted(set(blocks)), "block_edge_per_dtype": {
+            str(dt).replace("torch.", ""): sorted({blocks[v] for v in range(len(vols)) if vols[v].dtype == dt})
+            for dt in (torch.uint8, torch.uint16, torch.float32)}, "block_warps": block_warps,
+            "candidates": tune["candidates"], "tune_s": t_tune},
         "generate_s": t_gen, "steps": steps, "plain_steps": psteps,
     }
     for e in exts:
@@ -777,7 +793,7 @@ def run_backward(ctx, stream, steps):
     return out
 
 
-def run_gyroid(ctx, stream, steps, n=2048):
+def run_gyroid(ctx, stream, steps, n=2048, fixed=False):
     """The large float32 workload: n^3 gyroid sin(kx)cos(ky) + sin(ky)cos(kz) +
     sin(kz)cos(kx), k = 2 pi 12, + N(0, 0.02) (seed 2), isovalue 0 (32 GiB at
     2048^3).  mtx_autotune picks the block edge, warps, staging and min/max
@@ -790,7 +806,11 @@ def run_gyroid(ctx, stream, steps, n=2048):
     torch.cuda.synchronize()
     t_gen = time.perf_counter() - t0
     t0 = time.perf_counter()
-    tune = api.autotune(ctx, vol, 0.0, flags=L.AUTOTUNE_QUICK)
+    default = {"minmaxZChunk": 0, "minmaxSlices": 0, "extractWarps": 0, "staging": 0, "extractCtasPerSm": 0}
+    if fixed:  # profiling runs: block 8, default tuning
+        tune = {"blockEdge": 8, "tuning": default, "candidates": 0}
+    else:
+        tune = api.autotune(ctx, vol, 0.0)  # best of three repetitions per candidate
     t_tune = time.perf_counter() - t0
 
     def timed(block, tuning):
@@ -811,12 +831,21 @@ def run_gyroid(ctx, stream, steps, n=2048):
         ctx.synchronize()
         c = ex.counters.cpu().numpy().view(np.uint32)
         assert int(c[4]) == 0 and int(c[0]) == V and int(c[1]) == 3 * T
+        # per-stage split of the same call (profiler events between the stages)
+        prof = api.Profiler(ctx)
+        ctx.set_profiler(prof)
+        prof.begin_frame()
+        for _ in range(3):
+            ex.run()
+        prof.end_frame()
+        ctx.set_profiler(None)
+        stages = {k: v[0] / 3 for k, v in prof.regions().items()}
+        prof.close()
         del ex
-        return e0.elapsed_time(e1) / steps, V, T, A
+        return e0.elapsed_time(e1) / steps, V, T, A, stages
 
-    default = {"minmaxZChunk": 0, "minmaxSlices": 0, "extractWarps": 0, "staging": 0}
-    ms_tuned, V, T, A = timed(tune["blockEdge"], tune["tuning"])
-    ms_default, V8, T8, _ = timed(8, default)
+    ms_tuned, V, T, A, stages = timed(tune["blockEdge"], tune["tuning"])
+    ms_default, V8, T8, _, _ = (ms_tuned, V, T, A, stages) if fixed else timed(8, default)
     ctx.set_tuning(0, 0, 0, 0)
     nvox = n ** 3
     peak, peak_kind = peak_hbm()
@@ -828,6 +857,7 @@ def run_gyroid(ctx, stream, steps, n=2048):
         "ms_tuned": ms_tuned, "ms_default_b8": ms_default, "speedup_vs_default": ms_default / ms_tuned,
         "gvoxels_per_s": nvox / ms_tuned / 1e6, "tris_per_s": T / ms_tuned * 1e3,
         "vertices": V, "triangles": T, "active_blocks": A, "triangles_b8": T8,
+        "stages_ms": stages,
         "pipeline_roofline": {"achieved": alg / ms_tuned / 1e6, "peak": peak, "unit": "GB/s",
                               "frac": alg / ms_tuned / 1e6 / peak, "algorithmic_bytes": alg, "peak_kind": peak_kind,
                               "what": "volume read once + 12 B per vertex + 12 B per triangle written"},
@@ -851,6 +881,8 @@ def main():
     ap.add_argument("--batch-scale", type=int, default=1, help="divide the batch's volume edges (profiling runs only)")
     ap.add_argument("--no-gyroid", action="store_true", help="skip the autotuned 2048^3 float32 gyroid leg")
     ap.add_argument("--gyroid-size", type=int, default=2048, help="gyroid edge (profiling runs only)")
+    ap.add_argument("--gyroid-fixed", action="store_true", help="gyroid at block 8, no autotuner (profiling runs only)")
+    ap.add_argument("--batch-fixed", action="store_true", help="batch at block 8, no autotuner (profiling runs only)")
     ap.add_argument("--size", type=int, default=1024, help="volume edge (profiling runs only)")
     ap.add_argument("--cache", default="", help="raw file to read/write the generated volume")
     args = ap.parse_args()

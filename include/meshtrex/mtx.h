@@ -466,6 +466,8 @@ typedef struct mtx_batch_desc {
     uint32_t frame;        /* mtx_frame */
     uint32_t normals;      /* MTX_VERTEX_DATA only */
     uint32_t useGraph;     /* 1 = record the run into a CUDA graph at the first mtx_batch_run */
+    uint32_t blockWarps;   /* warps of each CTA of the persistent kernel that take blocks, 1..8 (0 = as many
+                              as the shared memory holds, at most 8); fewer gives more CTAs an SM */
 } mtx_batch_desc;
 
 /* One job's slice of the pooled outputs. */
@@ -559,6 +561,28 @@ typedef struct mtx_autotune_result {
  * (extractionPipeline.cpp:238-256, pmb.task.glsl:19,27). */
 mtx_status mtx_autotune(mtx_context_t ctx, const mtx_volume *vol, float isovalue, const char *cache_path,
                         uint32_t flags, mtx_autotune_result *out);
+
+/* Result of mtx_autotune_batch (the per-volume block edges go to the
+ * caller's array). */
+typedef struct mtx_batch_autotune_result {
+    uint32_t blockWarps; /* for mtx_batch_desc::blockWarps (0 = as many as fit) */
+    uint32_t fromCache;  /* 1 if no candidate was timed */
+    uint32_t candidates; /* candidates timed */
+    uint32_t _pad;
+    double ms;           /* device time of one batched run with these choices */
+} mtx_batch_autotune_result;
+
+/* Picks, for a batch, the block edge of every volume (4, 8 or 16, written to
+ * blockEdges[volumeCount]) and the batched kernel's block warps by timing the
+ * batched run itself on the device: one edge for all volumes at two warp
+ * counts, then each dtype's volumes moved to the other edges.  desc's own
+ * blockEdges, capacities, blockWarps and useGraph are ignored.  The choice
+ * is cached per (the batch's (dims, dtype) list, device name) in the process
+ * and, when cache_path is not NULL, appended to that text file, which later
+ * calls and processes read first.  flags as mtx_autotune.  No meshtrex
+ * counterpart. */
+mtx_status mtx_autotune_batch(mtx_context_t ctx, const mtx_batch_desc *desc, const char *cache_path,
+                              uint32_t flags, uint32_t *blockEdges, mtx_batch_autotune_result *out);
 
 /* Records the stage times of every later call on this context that is not
  * given its own profiler, the asynchronous whole-path call included (NULL

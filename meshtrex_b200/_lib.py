@@ -84,6 +84,11 @@ class Tuning(C.Structure):
                 ("extractWarps", C.c_uint32), ("staging", C.c_uint32), ("extractCtasPerSm", C.c_uint32)]
 
 
+class BatchAutotuneResult(C.Structure):
+    _fields_ = [("blockWarps", C.c_uint32), ("fromCache", C.c_uint32), ("candidates", C.c_uint32),
+                ("_pad", C.c_uint32), ("ms", C.c_double)]
+
+
 class MeshBuffers(C.Structure):
     _fields_ = [("vertices", C.c_void_p), ("vertexCapacity", C.c_uint64),
                 ("indices", C.c_void_p), ("triangleCapacity", C.c_uint64),
@@ -107,7 +112,7 @@ class BatchDesc(C.Structure):
                 ("jobs", C.POINTER(BatchJob)), ("maxActiveBlocks", C.c_uint64),
                 ("vertexCapacity", C.c_uint64), ("triangleCapacity", C.c_uint64),
                 ("vertexFormat", C.c_uint32), ("frame", C.c_uint32), ("normals", C.c_uint32),
-                ("useGraph", C.c_uint32)]
+                ("useGraph", C.c_uint32), ("blockWarps", C.c_uint32)]
 
 
 class BatchJobResult(C.Structure):
@@ -194,6 +199,8 @@ SIGNATURES = [
     ("mtx_context_set_tuning", _ST, [_P, C.POINTER(Tuning)]),
     ("mtx_context_get_tuning", _ST, [_P, C.POINTER(Tuning)]),
     ("mtx_autotune", _ST, [_P, C.POINTER(Volume), C.c_float, C.c_char_p, C.c_uint32, C.POINTER(AutotuneResult)]),
+    ("mtx_autotune_batch", _ST, [_P, C.POINTER(BatchDesc), C.c_char_p, C.c_uint32, C.POINTER(C.c_uint32),
+                                 C.POINTER(BatchAutotuneResult)]),
     ("mtx_profiler_destroy", _ST, [_P]),
     ("mtx_profiler_begin_frame", _ST, [_P]),
     ("mtx_profiler_end_frame", _ST, [_P]),

@@ -455,7 +455,7 @@ class Batch:
 
     def __init__(self, ctx: Context, volumes, blocks, jobs, max_active_blocks: int = 0,
                  vertex_capacity: int = 0, triangle_capacity: int = 0,
-                 options: L.ExtractOptions | None = None, use_graph: bool = True):
+                 options: L.ExtractOptions | None = None, use_graph: bool = True, block_warps: int = 0):
         self.ctx = ctx
         self.volumes = list(volumes)  # keeps the tensors alive
         self._vols = (L.Volume * len(self.volumes))(*[wrap_volume(v) for v in self.volumes])
@@ -476,6 +476,7 @@ class Batch:
         d.frame = opts.frame
         d.normals = opts.normals
         d.useGraph = 1 if use_graph else 0
+        d.blockWarps = int(block_warps)
         self.handle = C.c_void_p()
         L.check(L.lib().mtx_batch_create(ctx.handle, C.byref(d), C.byref(self.handle)), "mtx_batch_create",
                 ctx.handle)
@@ -529,3 +530,27 @@ def autotune(ctx: Context, volume: torch.Tensor, iso: float, cache_path: str | N
             "mtx_autotune", ctx.handle)
     t = {f: getattr(r.tuning, f) for f, _ in L.Tuning._fields_}
     return {"blockEdge": r.blockEdge, "tuning": t, "ms": r.ms, "fromCache": r.fromCache, "candidates": r.candidates}
+
+
+def autotune_batch(ctx: Context, volumes, jobs, cache_path: str | None = None, flags: int = 0) -> dict:
+    """mtx_autotune_batch: the block edge of every volume and the batched
+    kernel's block warps for the batch (volumes: CUDA tensors [z, y, x]; jobs:
+    (volume index, isovalue)), timed on the batched run itself.  Returns
+    {blockEdges: [...], blockWarps, ms, fromCache, candidates}."""
+    vols = list(volumes)
+    nv = len(vols)
+    d = L.BatchDesc()
+    arr = (L.Volume * nv)(*[wrap_volume(v) for v in vols])
+    edges = (C.c_uint32 * nv)(*([8] * nv))
+    jarr = (L.BatchJob * len(jobs))(*[L.BatchJob(int(v), float(i)) for v, i in jobs])
+    d.volumeCount = nv
+    d.jobCount = len(jobs)
+    d.volumes = arr
+    d.blockEdges = edges
+    d.jobs = jarr
+    out_edges = (C.c_uint32 * nv)()
+    r = L.BatchAutotuneResult()
+    L.check(L.lib().mtx_autotune_batch(ctx.handle, C.byref(d), cache_path.encode() if cache_path else None,
+                                       int(flags), out_edges, C.byref(r)), "mtx_autotune_batch", ctx.handle)
+    return {"blockEdges": list(out_edges), "blockWarps": r.blockWarps, "ms": r.ms, "fromCache": r.fromCache,
+            "candidates": r.candidates}

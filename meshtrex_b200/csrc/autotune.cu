@@ -186,3 +186,229 @@ extern "C" mtx_status mtx_autotune(mtx_context_t c, const mtx_volume *vol, float
     out->candidates = tried;
     return MTX_OK;
 }
+
+// ------------------------------------------------------------- batches
+// mtx_autotune_batch: the block edge of every volume of a batch and the
+// batched kernel's block warps, by timing the batched run itself (the plain
+// path's best edge does not carry over: the batched bodies at edge 4 take
+// twice the time of edge 8 on dense blob volumes).  Candidates: one edge for
+// every volume (4, 8, 16) at 8 and 6 block warps; then, from the best, each
+// dtype's volumes moved to the other edges in turn.  A candidate is run once
+// with small capacities to learn the sizes it needs, then created with those,
+// run once to warm up and timed (CUDA events on the context's stream), best
+// of `reps`.  Cached per (the batch's sorted (dims, dtype) list, device name):
+// in memory and, given a path, as lines
+//   batch <edges of the volumes in the order of the list> <warps> <ms> <key>
+namespace {
+
+struct BatchEntry {
+    std::vector<uint32_t> edges;  // per volume, in the order of the sorted key
+    uint32_t warps;
+    double ms;
+};
+std::map<std::string, BatchEntry> g_batch_cache;
+
+// The key: "X,Y,Z,dtype;" per volume in sorted order, then the device name;
+// order[i] is the volume behind the i-th entry.
+std::string batch_key(const mtx_batch_desc *d, const char *device, std::vector<uint32_t> &order) {
+    std::vector<std::pair<std::string, uint32_t>> v;
+    for (uint32_t i = 0; i < d->volumeCount; ++i) {
+        const mtx_volume &m = d->volumes[i];
+        v.push_back({std::to_string(m.dims[0]) + "," + std::to_string(m.dims[1]) + "," + std::to_string(m.dims[2]) +
+                         "," + std::to_string(m.dtype) + ";",
+                     i});
+    }
+    std::stable_sort(v.begin(), v.end());
+    std::string k;
+    order.clear();
+    for (auto &e : v) {
+        k += e.first;
+        order.push_back(e.second);
+    }
+    return k + device;
+}
+
+bool read_batch_file(const char *path, const std::string &key, size_t n, BatchEntry &e) {
+    FILE *f = path ? fopen(path, "r") : nullptr;
+    if (!f) return false;
+    std::string line;
+    bool found = false;
+    char buf[1 << 16];
+    while (fgets(buf, sizeof(buf), f)) {
+        line = buf;
+        if (line.compare(0, 6, "batch ") != 0) continue;
+        if (!line.empty() && line.back() == '\n') line.pop_back();
+        const char *s = line.c_str() + 6;
+        BatchEntry t;
+        bool ok = true;
+        for (size_t i = 0; i < n && ok; ++i) {
+            char *end;
+            const unsigned long x = strtoul(s, &end, 10);
+            ok = end != s;
+            t.edges.push_back((uint32_t)x);
+            s = end;
+        }
+        char *end;
+        t.warps = ok ? (uint32_t)strtoul(s, &end, 10) : 0;
+        if (ok) {
+            s = end;
+            t.ms = strtod(s, &end);
+            s = end;
+            while (*s == ' ') ++s;
+            if (key == s) {
+                e = t;
+                found = true;
+            }
+        }
+    }
+    fclose(f);
+    return found;
+}
+
+void append_batch_file(const char *path, const std::string &key, const BatchEntry &e) {
+    FILE *f = path ? fopen(path, "a") : nullptr;
+    if (!f) return;
+    fprintf(f, "batch");
+    for (uint32_t x : e.edges) fprintf(f, " %u", x);
+    fprintf(f, " %u %.6f %s\n", e.warps, e.ms, key.c_str());
+    fclose(f);
+}
+
+// Device time of one batched run of `d` with these block edges and warps.
+mtx_status time_batch(mtx_context *c, const mtx_batch_desc *d, const std::vector<uint32_t> &edges, uint32_t warps,
+                      uint32_t reps, double &best) {
+    mtx_batch_desc t = *d;
+    t.blockEdges = edges.data();
+    t.blockWarps = warps;
+    t.useGraph = 0;
+    // sizes: runs with small capacities report what the run needs -- the
+    // active blocks first, then (with room for those) the vertices and triangles
+    t.maxActiveBlocks = 1u << 16;
+    t.vertexCapacity = t.triangleCapacity = 1u << 16;
+    mtx_batch_t b = nullptr;
+    mtx_status rs = MTX_OK;
+    mtx_batch_totals tot{};
+    for (int pass = 0; pass < 2 && rs == MTX_OK; ++pass) {
+        if ((rs = mtx_batch_create(c, &t, &b)) != MTX_OK) return rs;
+        rs = mtx_batch_run(b);
+        if (rs == MTX_OK) {
+            rs = mtx_batch_read_results(b, nullptr, &tot);
+            if (rs == MTX_ERR_CAPACITY) rs = MTX_OK;
+        }
+        mtx_batch_destroy(b);
+        t.maxActiveBlocks = std::max<uint64_t>(tot.activeBlocks, 1);
+    }
+    if (rs != MTX_OK) return rs;
+    t.maxActiveBlocks = std::max<uint64_t>(tot.activeBlocks, 1);
+    t.vertexCapacity = std::max<uint64_t>(tot.vertexCount, 1);
+    t.triangleCapacity = std::max<uint64_t>(tot.triangleCount, 1);
+    if ((rs = mtx_batch_create(c, &t, &b)) != MTX_OK) return rs;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    best = 1e30;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) rs = MTX_ERR_CUDA;
+    if (rs == MTX_OK) rs = mtx_batch_run(b);  // warm-up
+    for (uint32_t r = 0; r < reps && rs == MTX_OK; ++r) {
+        cudaEventRecord(e0, c->stream);
+        rs = mtx_batch_run(b);
+        cudaEventRecord(e1, c->stream);
+        if (rs == MTX_OK) rs = mtx_batch_read_results(b, nullptr, nullptr);
+        float ms = 0.0f;
+        if (rs == MTX_OK && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) best = std::min(best, (double)ms);
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    mtx_batch_destroy(b);
+    return rs;
+}
+
+}  // namespace
+
+extern "C" mtx_status mtx_autotune_batch(mtx_context_t c, const mtx_batch_desc *d, const char *cache_path,
+                                         uint32_t flags, uint32_t *blockEdges, mtx_batch_autotune_result *out) {
+    if (!c || !d || !blockEdges || !out || !d->volumes || !d->volumeCount || !d->jobs || !d->jobCount)
+        return c ? fail(c, MTX_ERR_INVALID_ARG, "null argument") : MTX_ERR_INVALID_ARG;
+    DeviceGuard dg(c->device);
+    join_extract(c);
+    memset(out, 0, sizeof(*out));
+    cudaDeviceProp prop;
+    MTX_CUDA(c, cudaGetDeviceProperties(&prop, c->device));
+    std::vector<uint32_t> order;
+    const std::string key = batch_key(d, prop.name, order);
+    const uint32_t n = d->volumeCount;
+    BatchEntry e;
+    bool hit = false;
+    if (!(flags & MTX_AUTOTUNE_IGNORE_CACHE)) {
+        std::lock_guard<std::mutex> lk(g_mu);
+        auto it = g_batch_cache.find(key);
+        if (it != g_batch_cache.end()) {
+            e = it->second;
+            hit = true;
+        } else if (read_batch_file(cache_path, key, n, e)) {
+            g_batch_cache[key] = e;
+            hit = true;
+        }
+    }
+    if (hit) {
+        for (uint32_t i = 0; i < n; ++i) blockEdges[order[i]] = e.edges[i];
+        out->blockWarps = e.warps;
+        out->ms = e.ms;
+        out->fromCache = 1;
+        return MTX_OK;
+    }
+    const uint32_t reps = (flags & MTX_AUTOTUNE_QUICK) ? 1u : 3u;
+    mtx_status rs = MTX_OK;
+    std::vector<uint32_t> best_edges(n, 8), edges(n);
+    uint32_t best_warps = 0, tried = 0;
+    double best = 1e30;
+    auto consider = [&](const std::vector<uint32_t> &ed, uint32_t w) {
+        double ms;
+        rs = time_batch(c, d, ed, w, reps, ms);
+        if (rs != MTX_OK) return;
+        ++tried;
+        if (ms < best) {
+            best = ms;
+            best_edges = ed;
+            best_warps = w;
+        }
+    };
+    // one edge for every volume, at 8 (as many as fit) and 6 block warps
+    for (uint32_t B : {4u, 8u, 16u})
+        for (uint32_t w : {0u, 6u}) {
+            if (rs != MTX_OK) break;
+            std::fill(edges.begin(), edges.end(), B);
+            consider(edges, w);
+        }
+    // then each dtype's volumes at the other edges
+    for (uint32_t dt = 0; dt <= MTX_DTYPE_F32 && rs == MTX_OK; ++dt) {
+        bool any = false;
+        for (uint32_t i = 0; i < n; ++i) any |= d->volumes[i].dtype == dt;
+        if (!any) continue;
+        const std::vector<uint32_t> base = best_edges;
+        for (uint32_t B : {4u, 8u, 16u}) {
+            edges = base;
+            bool changed = false;
+            for (uint32_t i = 0; i < n; ++i)
+                if (d->volumes[i].dtype == dt && edges[i] != B) {
+                    edges[i] = B;
+                    changed = true;
+                }
+            if (changed) consider(edges, best_warps);
+            if (rs != MTX_OK) break;
+        }
+    }
+    if (rs != MTX_OK) return rs;
+    e.edges.resize(n);
+    for (uint32_t i = 0; i < n; ++i) e.edges[i] = best_edges[order[i]];
+    e.warps = best_warps;
+    e.ms = best;
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        g_batch_cache[key] = e;
+        append_batch_file(cache_path, key, e);
+    }
+    for (uint32_t i = 0; i < n; ++i) blockEdges[i] = best_edges[i];
+    out->blockWarps = best_warps;
+    out->ms = best;
+    out->candidates = tried;
+    return MTX_OK;
+}

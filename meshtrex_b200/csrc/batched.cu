@@ -831,6 +831,11 @@ mtx_status mtx_batch_create(mtx_context_t c, const mtx_batch_desc *d, mtx_batch_
     const int static_smem = 1024;
     const int room = (c->max_smem_optin > 0 ? c->max_smem_optin : 227 * 1024) - (int)kTableBytes - static_smem;
     a.block_warps = (uint32_t)std::min<int>(kBWarps, std::max(0, room / (int)L.bytes));
+    if (d->blockWarps > kBWarps) {
+        batch_release(b);
+        return fail(c, MTX_ERR_INVALID_ARG, "batch: blockWarps outside 0..8");
+    }
+    if (d->blockWarps) a.block_warps = std::min<uint32_t>(a.block_warps, d->blockWarps);
     if (a.block_warps == 0) {
         batch_release(b);
         return fail(c, MTX_ERR_UNSUPPORTED, "batch: warp layout does not fit shared memory");

@@ -65,3 +65,35 @@ def test_autotune_reads_a_cache_file_written_before(ctx, tmp_path):
     assert r["fromCache"] == 1 and r["blockEdge"] == 16 and r["ms"] == 1.25
     assert r["tuning"] == {"minmaxZChunk": 0, "minmaxSlices": 4, "extractWarps": 8, "staging": 2,
                            "extractCtasPerSm": 0}
+
+
+def test_batch_autotune_picks_edges_caches_them_and_matches_oracle(ctx, oracle, tmp_path):
+    """mtx_autotune_batch times the batched run for one edge for all volumes
+    (4, 8, 16) and per-dtype changes; the choice is cached per the batch's
+    (dims, dtype) list, read back from the file by a later call that ignores
+    nothing, and the batch with those edges gives the oracle's meshes."""
+    from helpers import blob_volume, mid_iso, to_cuda
+    from meshtrex_b200 import api
+    arrays = [blob_volume((24, 40, 32), np.uint8, seed=71), blob_volume((32, 24, 48), np.uint16, seed=72),
+              blob_volume((40, 32, 24), np.float32, seed=73)]
+    vols = [to_cuda(a) for a in arrays]
+    jobs = [(v, mid_iso(a)) for v, a in enumerate(arrays)] + [(0, float(np.percentile(arrays[0], 30)))]
+    cache = tmp_path / "batch_tune.txt"
+    r1 = api.autotune_batch(ctx, vols, jobs, cache_path=str(cache), flags=1)  # ignore any cached choice
+    assert r1["fromCache"] == 0 and r1["candidates"] >= 6 and r1["ms"] > 0
+    assert all(e in (4, 8, 16) for e in r1["blockEdges"]) and len(r1["blockEdges"]) == 3
+    assert r1["blockWarps"] in (0, 6)
+    r2 = api.autotune_batch(ctx, vols, jobs, cache_path=str(cache))
+    assert r2["fromCache"] == 1 and r2["blockEdges"] == r1["blockEdges"] and r2["blockWarps"] == r1["blockWarps"]
+    assert "batch " in cache.read_text()
+    b = api.Batch(ctx, vols, r1["blockEdges"], jobs, block_warps=r1["blockWarps"])
+    try:
+        b.run()
+        res, tot = b.results()
+        for (v, iso), r in zip(jobs, res):
+            ref = oracle.extract(arrays[v], r1["blockEdges"][v], iso)
+            gv, gi, _ = b.mesh(r)
+            np.testing.assert_array_equal(gv.cpu().numpy().view(np.uint32), ref.xyz.view(np.uint32))
+            np.testing.assert_array_equal(u32(gi), ref.indices)
+    finally:
+        b.close()
