@@ -468,12 +468,15 @@ def run_mtx(args):
     if not args.no_backward:
         line["backward"] = run_backward(ctx, stream, steps=max(3, min(20, steps)))
 
+    if not args.no_cpu and rank == 0:
+        line["blobs"] = run_blobs(ctx, stream, steps=max(3, min(20, steps)))
+
     if not args.no_gyroid:
         exts = vol = None  # release the 1024^3 volume and its outputs first
         torch.cuda.synchronize()
         torch.cuda.empty_cache()
         line["gyroid"] = run_gyroid(ctx, stream, steps=max(3, min(10, steps)), n=args.gyroid_size,
-                                    fixed=args.gyroid_fixed)
+                                    fixed=args.gyroid_fixed, with_cpu=not args.no_cpu and rank == 0)
 
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -715,6 +718,55 @@ def run_batched(ctx, stream, steps, scale_down=1, fixed=False):
     return out
 
 
+def run_blobs(ctx, stream, steps):
+    """The CPU-runnable plain workload: 256^3 uint8 Gaussian blobs + N(0, 4)
+    (seed 0), block 8^3, isovalue 128.  The asynchronous whole-path call timed
+    with CUDA events (the volume is 16 MiB, so L2 holds it: this leg is
+    latency-bound and reported beside the CPU path, not as the headline), and
+    the oracle's full mesh on the same host bytes on one thread and on all
+    host threads, checked against the GPU's bit for bit."""
+    from meshtrex_b200 import api, synth
+    from oracle import oracle as O
+    vol = synth.blobs(256, seed=0, device="cuda")
+    torch.cuda.synchronize()
+    host = vol.cpu().numpy()
+    ref = O.extract(host, 8, 128.0, nthreads=nproc())
+    ex = api.AsyncExtractor(ctx, vol, 8, 128.0, ref.n_vertices + 1, ref.n_triangles + 1,
+                            max_active_blocks=len(ref.ids) + 1)
+    for _ in range(3):
+        ex.run()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps):
+        ex.run()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    c = ex.counters.cpu().numpy().view(np.uint32)
+    V, T = int(c[0]), int(c[1]) // 3
+    match = (int(c[4]) == 0 and V == ref.n_vertices and T == ref.n_triangles
+             and np.array_equal(ex.vertices[:V].cpu().numpy().view(np.uint32), ref.xyz.view(np.uint32))
+             and np.array_equal(ex.indices[:T].cpu().numpy().view(np.uint32), ref.indices))
+
+    def cpu(threads):
+        secs, reps = 0.0, 0
+        while reps == 0 or (secs < 3.0 and reps < 50):
+            t0 = time.perf_counter()
+            O.extract(host, 8, 128.0, nthreads=threads)
+            secs += time.perf_counter() - t0
+            reps += 1
+        return host.size * reps / secs / 1e9
+    nvox = host.size
+    return {"workload": "256^3 uint8 Gaussian blobs + N(0, 4) (seed 0), block 8^3, isovalue 128",
+            "vertices": V, "triangles": T, "active_blocks": len(ref.ids), "ms": ms,
+            "gvoxels_per_s": nvox / ms / 1e6, "tris_per_s": T / ms * 1e3,
+            "pipeline_roofline_frac": (nvox + 12 * V + 12 * T) / ms / 1e6 / peak_hbm()[0],
+            "oracle_match": bool(match),
+            "cpu_1thread_gvoxels_per_s": cpu(1), "cpu_allcore_gvoxels_per_s": cpu(nproc()), "cpu_cores": nproc(),
+            "steps": steps}
+
+
 def run_backward(ctx, stream, steps):
     """The differentiation workload: 512^3 float32 torus SDF (R 0.3, r 0.1) +
     0.05 fBm (seed 4), isovalue 0, block 8^3.  Forward = the whole plain
@@ -793,7 +845,7 @@ def run_backward(ctx, stream, steps):
     return out
 
 
-def run_gyroid(ctx, stream, steps, n=2048, fixed=False):
+def run_gyroid(ctx, stream, steps, n=2048, fixed=False, with_cpu=False):
     """The large float32 workload: n^3 gyroid sin(kx)cos(ky) + sin(ky)cos(kz) +
     sin(kz)cos(kx), k = 2 pi 12, + N(0, 0.02) (seed 2), isovalue 0 (32 GiB at
     2048^3).  mtx_autotune picks the block edge, warps, staging and min/max
@@ -846,6 +898,19 @@ def run_gyroid(ctx, stream, steps, n=2048, fixed=False):
 
     ms_tuned, V, T, A, stages = timed(tune["blockEdge"], tune["tuning"])
     ms_default, V8, T8, _, _ = (ms_tuned, V, T, A, stages) if fixed else timed(8, default)
+    cpu = None
+    if with_cpu:  # the oracle on z-slabs of the same field, all host threads and one thread
+        from oracle import oracle as O
+        res = {}
+        for threads, nz in ((nproc(), 64), (1, 8)):
+            z0 = n // 2
+            slab = vol[z0:z0 + nz + 1].contiguous().cpu().numpy()
+            t0 = time.perf_counter()
+            O.extract(slab, tune["blockEdge"], 0.0, nthreads=threads)
+            res[threads] = slab.size / (time.perf_counter() - t0) / 1e9
+        cpu = {"allcore_gvoxels_per_s": res[nproc()], "1thread_gvoxels_per_s": res[1], "cores": nproc(),
+               "sample": f"z-slabs of {n}x{n}x65 (all threads) and {n}x{n}x9 (one thread) at the middle, the "
+                         "autotuned block edge, full mesh"}
     ctx.set_tuning(0, 0, 0, 0)
     nvox = n ** 3
     peak, peak_kind = peak_hbm()
@@ -857,7 +922,7 @@ def run_gyroid(ctx, stream, steps, n=2048, fixed=False):
         "ms_tuned": ms_tuned, "ms_default_b8": ms_default, "speedup_vs_default": ms_default / ms_tuned,
         "gvoxels_per_s": nvox / ms_tuned / 1e6, "tris_per_s": T / ms_tuned * 1e3,
         "vertices": V, "triangles": T, "active_blocks": A, "triangles_b8": T8,
-        "stages_ms": stages,
+        "stages_ms": stages, "cpu_baseline": cpu,
         "pipeline_roofline": {"achieved": alg / ms_tuned / 1e6, "peak": peak, "unit": "GB/s",
                               "frac": alg / ms_tuned / 1e6 / peak, "algorithmic_bytes": alg, "peak_kind": peak_kind,
                               "what": "volume read once + 12 B per vertex + 12 B per triangle written"},
