@@ -26,13 +26,18 @@ namespace mtx {
 constexpr bool kSingleBuffer = true;
 
 // ------------------------------------------------------------- count pass
-template <typename T, bool TMA>
+// BC: the block edge at compile time (0: p.B at run time).  The bench's edge 8
+// has its own instantiation, in which the warp's shared-memory plan and every
+// division by the edge fold to constants.
+template <typename T, bool TMA, int BC>
 __global__ void __launch_bounds__(kMaxWarps * 32)
-    pmb_count_kernel(Problem p, const __grid_constant__ CUtensorMap map, const uint32_t *__restrict__ ids,
+    pmb_count_kernel(Problem p_, const __grid_constant__ CUtensorMap map, const uint32_t *__restrict__ ids,
                      const uint32_t *__restrict__ count_ptr, mtx_meshlet_descriptor *__restrict__ desc,
                      uint64_t desc_cap, uint32_t *__restrict__ faces, uint8_t *__restrict__ state,
                      uint32_t *totals, uint8_t *__restrict__ cell_cases, uint64_t block_cap, DevStatus *st) {
     extern __shared__ __align__(128) unsigned char smem[];
+    Problem p = p_;
+    if (BC) p.B = BC;
     const WPlan pl = make_wplan(p.B, sizeof(T), TMA, false, kSingleBuffer, p.B <= 8);
     uint8_t *ntab = smem + 2048;
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, W = blockDim.x >> 5;
@@ -106,9 +111,9 @@ __global__ void __launch_bounds__(kScanThreads)
 // The xyz form of B <= 8 fits in 80 registers without spilling (72), so five
 // CTAs of four warps share an SM (107 registers allowed four); the other forms
 // would spill under that bound.
-template <typename T, int CPL, bool TMA, bool GENERIC>
+template <typename T, int CPL, bool TMA, bool GENERIC, int BC>
 __global__ void __launch_bounds__(kMaxWarps * 32, (!GENERIC && CPL == 8) ? 3 : 1)
-    pmb_emit_kernel(Problem p, const __grid_constant__ CUtensorMap map, const uint32_t *__restrict__ ids,
+    pmb_emit_kernel(Problem p_, const __grid_constant__ CUtensorMap map, const uint32_t *__restrict__ ids,
                     const uint32_t *__restrict__ rank_map, const uint32_t *__restrict__ count_ptr,
                     const mtx_meshlet_descriptor *__restrict__ desc, const uint32_t *__restrict__ faces,
                     const uint8_t *__restrict__ state, uint32_t *__restrict__ indices, uint64_t tcap,
@@ -117,6 +122,8 @@ __global__ void __launch_bounds__(kMaxWarps * 32, (!GENERIC && CPL == 8) ? 3 : 1
     // B <= 8 with TMA: the count pass's block state comes with each tile
     constexpr bool STATE = TMA && CPL == 8;
     extern __shared__ __align__(128) unsigned char smem[];
+    Problem p = p_;
+    if (BC) p.B = BC;
     const WPlan pl = make_wplan(p.B, sizeof(T), TMA, true, kSingleBuffer);
     uint64_t *tab = reinterpret_cast<uint64_t *>(smem);
     uint8_t *ntab = smem + 2048;
@@ -222,7 +229,8 @@ static mtx_status run_count(mtx_context *c, const Problem &p, const ExtractArgs 
                             uint32_t W, cudaStream_t s) {
     const WPlan pl = make_wplan(p.B, sizeof(T), tma, false, kSingleBuffer, p.B <= 8);
     const uint32_t smem = kTableBytes + W * pl.bytes;
-    auto k = tma ? pmb_count_kernel<T, true> : pmb_count_kernel<T, false>;
+    auto k = tma ? (p.B == 8 ? pmb_count_kernel<T, true, 8> : pmb_count_kernel<T, true, 0>)
+                 : pmb_count_kernel<T, false, 0>;
     unsigned grid;
     mtx_status r = grid_for(c, k, W * 32, smem, a.host_count, W, grid);
     if (r != MTX_OK) return r;
@@ -233,11 +241,11 @@ static mtx_status run_count(mtx_context *c, const Problem &p, const ExtractArgs 
     return MTX_OK;
 }
 
-template <typename T, int CPL, bool TMA>
+template <typename T, int CPL, bool TMA, int BC = 0>
 static void (*emit_fn(bool generic))(Problem, CUtensorMap, const uint32_t *, const uint32_t *, const uint32_t *,
                                      const mtx_meshlet_descriptor *, const uint32_t *, const uint8_t *, uint32_t *,
                                      uint64_t, uint64_t, void *, uint64_t, uint32_t, uint32_t, uint32_t, DevStatus *) {
-    return generic ? pmb_emit_kernel<T, CPL, TMA, true> : pmb_emit_kernel<T, CPL, TMA, false>;
+    return generic ? pmb_emit_kernel<T, CPL, TMA, true, BC> : pmb_emit_kernel<T, CPL, TMA, false, BC>;
 }
 
 template <typename T>
@@ -246,8 +254,9 @@ static mtx_status run_emit(mtx_context *c, const Problem &p, const ExtractArgs &
     const WPlan pl = make_wplan(p.B, sizeof(T), tma, true, kSingleBuffer);
     const uint32_t smem = cta_fixed_bytes(p.B, true) + W * pl.bytes;
     const bool generic = a.vertices && (a.vertex_format != MTX_VERTEX_XYZ || a.frame != MTX_FRAME_VOXEL);
-    auto k = p.B <= 8 ? (tma ? emit_fn<T, 8, true>(generic) : emit_fn<T, 8, false>(generic))
-                      : (tma ? emit_fn<T, 32, true>(generic) : emit_fn<T, 32, false>(generic));
+    auto k = p.B == 8 && tma ? emit_fn<T, 8, true, 8>(generic)
+             : p.B <= 8    ? (tma ? emit_fn<T, 8, true>(generic) : emit_fn<T, 8, false>(generic))
+                           : (tma ? emit_fn<T, 32, true>(generic) : emit_fn<T, 32, false>(generic));
     unsigned grid;
     mtx_status r = grid_for(c, k, W * 32, smem, a.host_count, W, grid);
     if (r != MTX_OK) return r;
