@@ -185,9 +185,9 @@ __global__ void __launch_bounds__(kMaxWarps * 32, (!GENERIC && CPL == 8) ? 3 : 1
             if (have_next && pl.nbuf == 2) tile_drain<TMA>(pl, ws, buf ^ 1u, parity);
             break;
         }
-        gather_finish<CPL>(pl, nb_vb, rec, ws);
+        gather_finish<CPL, CPL == 8>(pl, nb_vb, rec, ws, d.vertexOffset);
         emit_block<T, GENERIC, false, CPL == 8, STATE>(p, pl, ws, buf, g, d, tab, ntab, owner, indices, tcap,
-                                                       vertices, vcap, vfmt, frame, normals, st, r);
+                                                       vertices, vcap, vfmt, frame, normals, st, r, cmap);
         if (!have_next) break;
         if (pl.nbuf == 1) tile_issue<T, TMA>(pl, ws, buf, gn, &map, state_of(rn));
         else buf ^= 1u;

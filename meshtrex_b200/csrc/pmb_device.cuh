@@ -89,7 +89,7 @@ __host__ __device__ inline WPlan make_wplan(uint32_t B, uint32_t esz, bool tma, 
     p.tile_bytes = p.PX * p.B1 * p.B1 * esz;
     p.nbuf = (p.tile_bytes <= 4096 && !single_buffer) ? 2 : 1;
     // the emit pass puts its voxel table (build_vtab, B <= 8) in the tile's slot
-    const uint32_t slot = (tri_pass && B <= 8) ? std::max(p.tile_bytes, 2 * B * B * B) : p.tile_bytes;
+    const uint32_t slot = (tri_pass && B <= 8) ? std::max(p.tile_bytes, 3 * p.B1 * p.B1 * p.B1) : p.tile_bytes;
     uint32_t o = 0;
     for (uint32_t b = 0; b < 2; ++b) {
         p.off_tile[b] = o;
@@ -98,8 +98,10 @@ __host__ __device__ inline WPlan make_wplan(uint32_t B, uint32_t esz, bool tma, 
     if (p.nbuf == 1) p.off_tile[1] = p.off_tile[0];
     p.off_bar = o;
     o += 16;
+    if (tri_pass && B <= 8) o += 32;  // first vertex of the block and of its seven +x/+y/+z neighbours (emit)
     p.off_rows = o;
-    o = align_up(o + 4 * p.B1 * p.B1, 16);
+    // the emit pass with TMA and B <= 8 takes the count pass's block state and builds no rows
+    if (!(tri_pass && tma && B <= 8)) o = align_up(o + 4 * p.B1 * p.B1, 16);
     p.off_cross = o;
     o = align_up(o + 12 * p.BB, 16);
     p.off_vp = o;
@@ -119,8 +121,8 @@ __host__ __device__ inline WPlan make_wplan(uint32_t B, uint32_t esz, bool tma, 
         p.off_nm = o;
         o = align_up(o + p.nb3, 16);
     }
-    p.off_jobs = o;  // a window of packed jobs (triangles or vertices) in output order
-    o = align_up(o + 4 * kJobWin, 16);
+    p.off_jobs = o;  // a window of packed jobs (triangles or vertices) in output order: the emit pass only
+    if (tri_pass) o = align_up(o + 4 * kJobWin, 16);
     p.bytes = align_up(o, 128);
     return p;
 }
@@ -653,57 +655,63 @@ __device__ __forceinline__ uint32_t edge_vertex(uint32_t x, uint32_t y, uint32_t
     return base + __popc(m & ((1u << ax) - 1u));
 }
 
-// Voxel table of the block's own voxels for B <= 8, built in the tile's slot
-// once the vertices are written: entry (z*B + y)*B + x holds the voxel's first
-// vertex relative to the block (11 bits: at most 3 * 512) and its owned-edge
-// mask << 11.  Only voxels that own a cut edge are written; triangle corners
-// refer to no other.
-__device__ __forceinline__ void build_vtab(const WPlan &pl, const unsigned char *ws, uint16_t *vt) {
-    const uint32_t lane = threadIdx.x & 31, B = pl.B, BB = pl.BB, R = (BB + 31) / 32;
+// Unified vertex table over the block's (B+1)^3 voxels for B <= 8, built in
+// the tile's slot once the vertices are written: a 16-bit entry per voxel,
+// the first vertex of the voxel relative to its block's first vertex (11
+// bits) | the block's number c << 11 (0 = this block, 1-7 = the +x/+y/+z
+// neighbour dx | dy << 1 | dz << 2), then a mask byte per voxel with its
+// owned cut edges.  Own voxels come from the crossing rows; the context layer
+// from the packed gather (gather_finish<CPL, true>).  A triangle corner is
+// then one entry, one mask and one base word.  Only voxels that own a cut
+// edge are written; triangle corners refer to no other.
+__device__ __forceinline__ void build_utab(const WPlan &pl, unsigned char *ws, uint16_t *ut, uint8_t *um,
+                                           const uint32_t *cmap) {
+    const uint32_t lane = threadIdx.x & 31, B = pl.B, B1 = pl.B1, BB = pl.BB, R = (BB + 31) / 32;
     const uint32_t *cross = reinterpret_cast<const uint32_t *>(ws + pl.off_cross);
     const uint32_t *vp = reinterpret_cast<const uint32_t *>(ws + pl.off_vp);
     for (uint32_t k = 0; k < R; ++k) {
         const uint32_t q = lane * R + k;
         if (q >= BB) break;
         const uint32_t xc = cross[q], yc = cross[BB + q], zc = cross[2 * BB + q];
+        const uint32_t z = fdiv(q, pl.rB), y = q - z * B, row = (z * B1 + y) * B1;
         uint32_t any = xc | yc | zc, run = vp[q];
         while (any) {
             const uint32_t x = __ffs(any) - 1;
             any &= any - 1u;
             const uint32_t m = ((xc >> x) & 1u) | (((yc >> x) & 1u) << 1) | (((zc >> x) & 1u) << 2);
-            if (MTX_BC(q * B + x, B * BB, kBcVoxTab)) vt[q * B + x] = (uint16_t)(run | (m << 11));
+            if (MTX_BC(row + x, B1 * B1 * B1, kBcVoxTab)) {
+                ut[row + x] = (uint16_t)run;
+                um[row + x] = (uint8_t)m;
+            }
             run += __popc(m);
+        }
+    }
+    const uint32_t *nvid = reinterpret_cast<const uint32_t *>(ws + pl.off_nvid);
+    const uint8_t *nm = ws + pl.off_nm;
+    for (uint32_t j = lane; j < pl.nb3; j += 32) {
+        const uint32_t e = cmap[j];
+        const uint32_t ti = (((e >> 23) & 31u) * B1 + ((e >> 18) & 31u)) * B1 + ((e >> 13) & 31u);
+        if (MTX_BC(ti, B1 * B1 * B1, kBcVoxTab)) {
+            ut[ti] = (uint16_t)nvid[j];
+            um[ti] = nm[j];
         }
     }
     __syncwarp();
 }
 
-// edge_vertex with the block's own voxels looked up in the voxel table.
-__device__ __forceinline__ uint32_t edge_vertex_vt(uint32_t x, uint32_t y, uint32_t z, uint32_t e,
-                                                   const uint8_t *owner, const uint16_t *vt, const uint32_t *nvid,
-                                                   const uint8_t *nm, uint32_t B, uint32_t vbase, bool &bad) {
-    const uint32_t own = owner[e];
-    const uint32_t ux = x + (own & 1u), uy = y + ((own >> 1) & 1u), uz = z + ((own >> 2) & 1u);
-    const uint32_t ax = own >> 3;
-    uint32_t base, m;
-    if (ux < B && uy < B && uz < B) {
-        const uint32_t v = vt[(uz * B + uy) * B + ux];
-        base = vbase + (v & 0x7ffu);
-        m = v >> 11;
-    } else {
-        const uint32_t jx = ctx_index(B, ux, uy, uz);
-        if (!MTX_BC(jx, 3 * B * B + 3 * B + 1, kBcContext)) {
-            bad = true;
-            return 0;
-        }
-        base = nvid[jx];
-        m = nm[jx];
-    }
-    if (base == kNoVertex || !((m >> ax) & 1u)) {
+// The vertex id of cube edge e of the cell whose low corner is tile voxel ti,
+// from the unified table (build_utab); nbase: the eight block first vertices.
+__device__ __forceinline__ uint32_t edge_vertex_ut(uint32_t ti, uint32_t e, const uint8_t *owner, const uint16_t *ut,
+                                                   const uint8_t *um, const uint32_t *nbase, uint32_t B1, bool &bad) {
+    const uint32_t o = owner[e];
+    const uint32_t i = ti + (o & 1u) + ((o >> 1) & 1u) * B1 + ((o >> 2) & 1u) * B1 * B1, ax = o >> 3;
+    if (!MTX_BC(i, B1 * B1 * B1, kBcVoxTab)) {
         bad = true;
         return 0;
     }
-    return base + __popc(m & ((1u << ax) - 1u));
+    const uint32_t m = um[i], v = ut[i];
+    bad |= !((m >> ax) & 1u);
+    return nbase[v >> 11] + (v & 0x7ffu) + __popc(m & ((1u << ax) - 1u));
 }
 
 // -------------------------------------------------------------- scan pass
@@ -867,20 +875,30 @@ __device__ __forceinline__ void gather_issue_map(const Problem &p, const WPlan &
 
 // Turns the gathered records into first-vertex ids and owned-edge masks of the
 // context layer (nb_vb: lane c holds neighbour c's first vertex id).
-template <int CPL>
+// PACKED (B <= 8, the unified table of build_utab): each entry keeps the
+// neighbour-relative first vertex and the neighbour's number, rel | c << 11,
+// and lanes 0-7 store the first vertex of the block (vbase, entry 0) and of
+// its neighbours into the plan's eight base words.
+template <int CPL, bool PACKED = false>
 __device__ __forceinline__ void gather_finish(const WPlan &pl, uint32_t nb_vb, const uint32_t rec[CPL],
-                                              unsigned char *ws) {
+                                              unsigned char *ws, uint32_t vbase = 0) {
     const uint32_t lane = threadIdx.x & 31, nb3 = pl.nb3;
     uint32_t *nvid = reinterpret_cast<uint32_t *>(ws + pl.off_nvid);
     uint8_t *nm = ws + pl.off_nm;
+    if constexpr (PACKED) {
+        if (lane < 8) reinterpret_cast<uint32_t *>(ws + pl.off_bar + 16)[lane] = lane ? nb_vb : vbase;
+    }
 #pragma unroll
     for (uint32_t k = 0; k < CPL; ++k) {
         if (k * 32 >= nb3) continue;
         const uint32_t j = k * 32 + lane;
-        const uint32_t vb = __shfl_sync(0xffffffffu, nb_vb, (rec[k] >> 27) & 7u);
+        const uint32_t vb = PACKED ? 0u : __shfl_sync(0xffffffffu, nb_vb, (rec[k] >> 27) & 7u);
         if (j < nb3) {
             const bool present = rec[k] >> 31;
-            nvid[j] = present ? vb + (rec[k] & 0xffffffu) : kNoVertex;
+            if constexpr (PACKED)
+                nvid[j] = (rec[k] & 0x7ffu) | (((rec[k] >> 27) & 7u) << 11);
+            else
+                nvid[j] = present ? vb + (rec[k] & 0xffffffu) : kNoVertex;
             nm[j] = present ? (uint8_t)((rec[k] >> 24) & 7u) : (uint8_t)0;
         }
     }
@@ -943,7 +961,8 @@ __device__ __forceinline__ void emit_block(const Problem &p, const WPlan &pl, un
                                            const Geo &g, const mtx_meshlet_descriptor &d, const uint64_t *tab,
                                            const uint8_t *ntab, const uint8_t *owner, uint32_t *indices,
                                            uint64_t tcap, void *vertices, uint64_t vcap, uint32_t vfmt,
-                                           uint32_t frame, uint32_t normals, DevStatus *st, uint32_t r) {
+                                           uint32_t frame, uint32_t normals, DevStatus *st, uint32_t r,
+                                           const uint32_t *cmap = nullptr) {
     const uint32_t lane = threadIdx.x & 31, B = pl.B, BB = pl.BB;
     const uint32_t *cross = reinterpret_cast<const uint32_t *>(ws + pl.off_cross);
     const uint32_t *vp = reinterpret_cast<const uint32_t *>(ws + pl.off_vp);
@@ -974,7 +993,9 @@ __device__ __forceinline__ void emit_block(const Problem &p, const WPlan &pl, un
     const uint16_t *mmk = reinterpret_cast<const uint16_t *>(ws + pl.off_mm);
     const uint8_t *ck = ws + pl.off_case;
     uint16_t *vt = reinterpret_cast<uint16_t *>(ws + pl.off_tile[buf]);  // the tile is dead past the vertices
-    if constexpr (VT) build_vtab(pl, ws, vt);
+    uint8_t *um = ws + pl.off_tile[buf] + 2 * pl.B1 * pl.B1 * pl.B1;
+    const uint32_t *nbase = reinterpret_cast<const uint32_t *>(ws + pl.off_bar + 16);
+    if constexpr (VT) build_utab(pl, ws, vt, um, cmap);
     const uint32_t R = (BB + 31) / 32, nt = d.primitiveCount;
     bool bad = false;
     for (uint32_t w0 = 0; w0 < nt; w0 += kJobWin) {
@@ -1007,11 +1028,10 @@ __device__ __forceinline__ void emit_block(const Problem &p, const WPlan &pl, un
                 const uint64_t w = tab[job >> 16] >> (4 + 12 * t);
                 uint32_t *o = indices + 3ull * (tbase + w0 + b + lane);  // each lane its own 12 bytes
                 if constexpr (VT) {
-                    o[0] = edge_vertex_vt(x, y, z, (uint32_t)(w & 0xFu), owner, vt, nvid, nm, B, d.vertexOffset, bad);
-                    o[1] = edge_vertex_vt(x, y, z, (uint32_t)((w >> 4) & 0xFu), owner, vt, nvid, nm, B,
-                                          d.vertexOffset, bad);
-                    o[2] = edge_vertex_vt(x, y, z, (uint32_t)((w >> 8) & 0xFu), owner, vt, nvid, nm, B,
-                                          d.vertexOffset, bad);
+                    const uint32_t ti = (z * pl.B1 + y) * pl.B1 + x;
+                    o[0] = edge_vertex_ut(ti, (uint32_t)(w & 0xFu), owner, vt, um, nbase, pl.B1, bad);
+                    o[1] = edge_vertex_ut(ti, (uint32_t)((w >> 4) & 0xFu), owner, vt, um, nbase, pl.B1, bad);
+                    o[2] = edge_vertex_ut(ti, (uint32_t)((w >> 8) & 0xFu), owner, vt, um, nbase, pl.B1, bad);
                 } else {
                     o[0] = edge_vertex(x, y, z, (uint32_t)(w & 0xFu), owner, cross, vp, nvid, nm, B, BB,
                                        d.vertexOffset, bad);
