@@ -108,9 +108,10 @@ __global__ void __launch_bounds__(kScanThreads)
 
 // -------------------------------------------------------------- emit pass
 // CPL: context voxels per lane, ceil((3B^2 + 3B + 1) / 32): 8 covers B <= 8, 32 covers B <= 16.
-// The xyz form of B <= 8 fits in 80 registers without spilling (72), so five
-// CTAs of four warps share an SM (107 registers allowed four); the other forms
-// would spill under that bound.
+// The xyz form of B <= 8 is bounded to 85 registers (three CTAs of 256
+// threads); it uses 58 at the compile-time edge 8 and about 71 otherwise, with
+// no spills, so shared memory (about 30 KB a CTA of four warps) sets its seven
+// CTAs an SM.  The other forms would spill under that bound.
 template <typename T, int CPL, bool TMA, bool GENERIC, int BC>
 __global__ void __launch_bounds__(kMaxWarps * 32, (!GENERIC && CPL == 8) ? 3 : 1)
     pmb_emit_kernel(Problem p_, const __grid_constant__ CUtensorMap map, const uint32_t *__restrict__ ids,

@@ -88,7 +88,7 @@ __host__ __device__ inline WPlan make_wplan(uint32_t B, uint32_t esz, bool tma, 
     p.PX = tile_pitch(B, esz, tma);
     p.tile_bytes = p.PX * p.B1 * p.B1 * esz;
     p.nbuf = (p.tile_bytes <= 4096 && !single_buffer) ? 2 : 1;
-    // the emit pass puts its voxel table (build_vtab, B <= 8) in the tile's slot
+    // the emit pass puts its vertex table (build_utab, B <= 8) in the tile's slot
     const uint32_t slot = (tri_pass && B <= 8) ? std::max(p.tile_bytes, 3 * p.B1 * p.B1 * p.B1) : p.tile_bytes;
     uint32_t o = 0;
     for (uint32_t b = 0; b < 2; ++b) {
@@ -954,7 +954,7 @@ __device__ __forceinline__ void count_block(const Problem &p, const WPlan &pl, u
 // Emit body of one block whose tile is staged and whose context layer has
 // been gathered: its own vertices (when `vertices` is set) and its triangles.
 // ANY as in emit_vertices.  VT: resolve triangle corners through the voxel
-// table (build_vtab; B <= 8 only).  STATE: the count pass's block state came
+// table (build_utab; B <= 8 only).  STATE: the count pass's block state came
 // with the tile (tile_issue), so the rows and counts are not rebuilt.
 template <typename T, bool GENERIC, bool ANY = false, bool VT = false, bool STATE = false>
 __device__ __forceinline__ void emit_block(const Problem &p, const WPlan &pl, unsigned char *ws, uint32_t buf,
