@@ -399,10 +399,15 @@ __device__ __forceinline__ void block_counts(const Problem &p, const WPlan &pl, 
             if (cases_out)
                 for (uint32_t x = 0; x < B; ++x) cases_out[q * B + x] = ((inside >> x) & 1u) ? 255 : 0;
             if (keep) reinterpret_cast<uint16_t *>(ws + pl.off_mm)[q] = (uint16_t)mm;
+            // the four rows of the cell row, read once for all its mixed cells
+            const uint32_t r00 = mm ? rows[z * pl.B1 + y] : 0u, r01 = mm ? rows[z * pl.B1 + y + 1] : 0u;
+            const uint32_t r10 = mm ? rows[(z + 1) * pl.B1 + y] : 0u, r11 = mm ? rows[(z + 1) * pl.B1 + y + 1] : 0u;
             while (mm) {
                 const uint32_t x = __ffs(mm) - 1;
                 mm &= mm - 1u;
-                const uint32_t cfg = cell_case(rows, pl.B1, x, y, z);
+                const uint32_t a = r00 >> x, b = r01 >> x, c = r10 >> x, e = r11 >> x;
+                const uint32_t cfg = (a & 3u) | ((b & 2u) << 1) | ((b & 1u) << 3) | ((c & 3u) << 4) | ((e & 2u) << 5) |
+                                     ((e & 1u) << 7);
                 stri += ntab[cfg];
                 if (!MTX_BC(q * B + x, B * BB, kBcRows)) continue;
                 if (cases_out) cases_out[q * B + x] = (uint8_t)cfg;
@@ -548,20 +553,37 @@ __device__ __forceinline__ void emit_vertices(const Problem &p, const WPlan &pl,
     const bool xyz = !GENERIC || vfmt == MTX_VERTEX_XYZ;
     for (uint32_t w0 = 0; w0 < nv; w0 += kJobWin) {
         const uint32_t w1 = w0 + kJobWin;
-        for (uint32_t k = 0; k < R; ++k) {
-            const uint32_t q = lane * R + k;
-            if (q >= BB) break;
-            const uint32_t xc = cross[q], yc = cross[BB + q], zc = cross[2 * BB + q];
-            uint32_t j = vp[q];
-            if (j >= w1 || j + __popc(xc) + __popc(yc) + __popc(zc) <= w0) continue;
-            uint32_t any = xc | yc | zc;
-            while (any) {
-                const uint32_t x = __ffs(any) - 1;
-                any &= any - 1u;
-                const uint32_t base = (q * B + x);
-                if ((xc >> x) & 1u) { if (j >= w0 && j < w1) jobs[j - w0] = base; ++j; }
-                if ((yc >> x) & 1u) { if (j >= w0 && j < w1) jobs[j - w0] = base | (1u << 12); ++j; }
-                if ((zc >> x) & 1u) { if (j >= w0 && j < w1) jobs[j - w0] = base | (2u << 12); ++j; }
+        if (nv <= kJobWin) {  // one window (the common case): no window checks
+            for (uint32_t k = 0; k < R; ++k) {
+                const uint32_t q = lane * R + k;
+                if (q >= BB) break;
+                const uint32_t xc = cross[q], yc = cross[BB + q], zc = cross[2 * BB + q];
+                uint32_t j = vp[q], any = xc | yc | zc;
+                while (any) {
+                    const uint32_t x = __ffs(any) - 1;
+                    any &= any - 1u;
+                    const uint32_t base = (q * B + x);
+                    if ((xc >> x) & 1u) jobs[j++] = base;
+                    if ((yc >> x) & 1u) jobs[j++] = base | (1u << 12);
+                    if ((zc >> x) & 1u) jobs[j++] = base | (2u << 12);
+                }
+            }
+        } else {
+            for (uint32_t k = 0; k < R; ++k) {
+                const uint32_t q = lane * R + k;
+                if (q >= BB) break;
+                const uint32_t xc = cross[q], yc = cross[BB + q], zc = cross[2 * BB + q];
+                uint32_t j = vp[q];
+                if (j >= w1 || j + __popc(xc) + __popc(yc) + __popc(zc) <= w0) continue;
+                uint32_t any = xc | yc | zc;
+                while (any) {
+                    const uint32_t x = __ffs(any) - 1;
+                    any &= any - 1u;
+                    const uint32_t base = (q * B + x);
+                    if ((xc >> x) & 1u) { if (j >= w0 && j < w1) jobs[j - w0] = base; ++j; }
+                    if ((yc >> x) & 1u) { if (j >= w0 && j < w1) jobs[j - w0] = base | (1u << 12); ++j; }
+                    if ((zc >> x) & 1u) { if (j >= w0 && j < w1) jobs[j - w0] = base | (2u << 12); ++j; }
+                }
             }
         }
         __syncwarp();
@@ -1000,20 +1022,38 @@ __device__ __forceinline__ void emit_block(const Problem &p, const WPlan &pl, un
     bool bad = false;
     for (uint32_t w0 = 0; w0 < nt; w0 += kJobWin) {
         const uint32_t w1 = w0 + kJobWin;
-        for (uint32_t k = 0; k < R; ++k) {
-            const uint32_t q = lane * R + k;
-            if (q >= BB) break;
-            uint32_t j = tp[q];
-            const uint32_t jend = (q + 1 < BB) ? tp[q + 1] : nt;
-            if (j >= w1 || jend <= w0) continue;
-            uint32_t mm = mmk[q];
-            while (mm) {
-                const uint32_t x = __ffs(mm) - 1;
-                mm &= mm - 1u;
-                const uint32_t cfg = ck[q * B + x];
-                const uint32_t n = ntab[cfg];
-                for (uint32_t t = 0; t < n; ++t, ++j)
-                    if (j >= w0 && j < w1) jobs[j - w0] = (q * B + x) | (t << 12) | (cfg << 16);
+        if (nt <= kJobWin) {  // one window (the common case): no window checks
+            for (uint32_t k = 0; k < R; ++k) {
+                const uint32_t q = lane * R + k;
+                if (q >= BB) break;
+                uint32_t j = tp[q], mm = mmk[q];
+                while (mm) {
+                    const uint32_t x = __ffs(mm) - 1;
+                    mm &= mm - 1u;
+                    const uint32_t cfg = ck[q * B + x];
+                    const uint32_t n = ntab[cfg], job = (q * B + x) | (cfg << 16);
+#pragma unroll
+                    for (uint32_t t = 0; t < 5; ++t)  // at most five triangles a case
+                        if (t < n) jobs[j + t] = job | (t << 12);
+                    j += n;
+                }
+            }
+        } else {
+            for (uint32_t k = 0; k < R; ++k) {
+                const uint32_t q = lane * R + k;
+                if (q >= BB) break;
+                uint32_t j = tp[q];
+                const uint32_t jend = (q + 1 < BB) ? tp[q + 1] : nt;
+                if (j >= w1 || jend <= w0) continue;
+                uint32_t mm = mmk[q];
+                while (mm) {
+                    const uint32_t x = __ffs(mm) - 1;
+                    mm &= mm - 1u;
+                    const uint32_t cfg = ck[q * B + x];
+                    const uint32_t n = ntab[cfg];
+                    for (uint32_t t = 0; t < n; ++t, ++j)
+                        if (j >= w0 && j < w1) jobs[j - w0] = (q * B + x) | (t << 12) | (cfg << 16);
+                }
             }
         }
         __syncwarp();
