@@ -39,6 +39,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32)
     Problem p = p_;
     if (BC) p.B = BC;
     const WPlan pl = make_wplan(p.B, sizeof(T), TMA, false, kSingleBuffer, p.B <= 8);
+    const GridDiv dv = grid_div(p);
     uint8_t *ntab = smem + 2048;
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, W = blockDim.x >> 5;
     unsigned char *ws = smem + kTableBytes + warp * pl.bytes;
@@ -65,7 +66,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32)
     uint32_t r = gw;
     Geo g{};
     if (r < count) {
-        g = block_geo(__ldg(ids + r), p, TMA, sizeof(T));
+        g = block_geo(__ldg(ids + r), p, TMA, sizeof(T), dv);
         tile_issue<T, TMA>(pl, ws, buf, g, &map);
     }
     while (r < count) {
@@ -73,7 +74,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32)
         Geo gn{};
         const bool have_next = rn < count;
         if (have_next) {
-            gn = block_geo(__ldg(ids + rn), p, TMA, sizeof(T));
+            gn = block_geo(__ldg(ids + rn), p, TMA, sizeof(T), dv);
             if (pl.nbuf == 2) tile_issue<T, TMA>(pl, ws, buf ^ 1u, gn, &map);
         }
         if (!tile_wait<T, TMA>(p, pl, ws, buf, g, parity, st)) {
@@ -126,6 +127,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32, (!GENERIC && CPL == 8) ? 3 : 1
     Problem p = p_;
     if (BC) p.B = BC;
     const WPlan pl = make_wplan(p.B, sizeof(T), TMA, true, kSingleBuffer);
+    const GridDiv dv = grid_div(p);
     uint64_t *tab = reinterpret_cast<uint64_t *>(smem);
     uint8_t *ntab = smem + 2048;
     uint8_t *owner = smem + 2048 + 256;
@@ -159,7 +161,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32, (!GENERIC && CPL == 8) ? 3 : 1
     };
     if (r < count) {
         const uint32_t id = __ldg(ids + r);
-        g = block_geo(id, p, TMA, sizeof(T));
+        g = block_geo(id, p, TMA, sizeof(T), dv);
         tile_issue<T, TMA>(pl, ws, buf, g, &map, state_of(r));
         d = desc[r];
         nb_rk = neighbour_rank(p, g, id, rank_map);
@@ -173,7 +175,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32, (!GENERIC && CPL == 8) ? 3 : 1
         uint32_t nb_rk_n = kNoVertex;
         if (have_next) {
             const uint32_t idn = __ldg(ids + rn);
-            gn = block_geo(idn, p, TMA, sizeof(T));
+            gn = block_geo(idn, p, TMA, sizeof(T), dv);
             if (pl.nbuf == 2) tile_issue<T, TMA>(pl, ws, buf ^ 1u, gn, &map, state_of(rn));
             dn = desc[rn];
             nb_rk_n = neighbour_rank(p, gn, idn, rank_map);

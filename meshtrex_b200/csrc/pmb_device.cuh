@@ -138,6 +138,41 @@ struct Geo {
     uint32_t xoff;        // tile column of the block's first voxel
 };
 
+// Exact division of a block id by the grid's row and slice sizes through a
+// 64-bit reciprocal and one high multiply (Lemire's method: m = floor((2^64 - 1)
+// / d) + 1 gives floor(a / d) = high 64 bits of m * a for every 32-bit a; d = 1
+// is taken apart), computed once per thread instead of two integer divisions
+// per block.
+struct GridDiv {
+    uint64_t mx, mxy;
+    uint32_t dx, dxy;
+};
+__device__ __forceinline__ GridDiv grid_div(const Problem &p) {
+    GridDiv d;
+    d.dx = p.GX;
+    d.dxy = p.GX * p.GY;
+    d.mx = d.dx > 1 ? ~0ull / d.dx + 1 : 0;
+    d.mxy = d.dxy > 1 ? ~0ull / d.dxy + 1 : 0;
+    return d;
+}
+__device__ __forceinline__ uint32_t div_by(uint32_t a, uint64_t m, uint32_t d) {
+    return d > 1 ? (uint32_t)__umul64hi(m, a) : a;
+}
+
+__device__ __forceinline__ Geo block_geo(uint32_t id, const Problem &p, bool tma, uint32_t esz, const GridDiv &dv) {
+    Geo g;
+    g.bz = div_by(id, dv.mxy, dv.dxy);
+    const uint32_t rest = id - g.bz * dv.dxy;
+    g.by = div_by(rest, dv.mx, dv.dx);
+    g.bx = rest - g.by * dv.dx;
+    g.ox = g.bx * p.B;
+    g.oy = g.by * p.B;
+    g.oz = g.bz * p.B;
+    g.nx = min(p.B, p.X - g.ox);
+    g.xoff = tma ? (g.ox % (16 / esz)) : 0u;
+    return g;
+}
+
 __device__ __forceinline__ Geo block_geo(uint32_t id, const Problem &p, bool tma, uint32_t esz) {
     Geo g;
     g.bx = id % p.GX;
