@@ -41,6 +41,7 @@ constexpr uint32_t kPhaseSpinLimit = 1u << 26;  // about 17 s of polling at the 
 struct BVol {
     Problem p;      // isovalue unset
     WPlan pl;       // region sizes of this volume, offsets of the batch's shared warp layout
+    GridDiv dv;     // reciprocals of the grid's row and slice sizes (block_geo)
     uint32_t vec;   // min/max by 16-byte vector warps (1) or one thread per block (0)
     uint32_t nXS, zchunk, pad;
     uint64_t leaf_off;  // first leaf entry of the volume in the pooled leaf array
@@ -450,18 +451,19 @@ __device__ __forceinline__ void batch_bases(const BatchArgs &a, uint32_t n, uint
 // the balanced ones (pmb_balanced.cuh): batches of many volumes and
 // isovalues tend to have dense blocks.
 __device__ __forceinline__ void batch_count_block(const BatchArgs &a, const Problem &p, const WPlan &pl,
-                                                  unsigned char *ws, const uint8_t *ntab, uint32_t id, uint32_t r) {
-    const Geo g = block_geo(id, p, false, 4);
+                                                  const GridDiv &dv, unsigned char *ws, const uint8_t *ntab,
+                                                  uint32_t id, uint32_t r) {
+    const Geo g = block_geo(id, p, false, 4, dv);
     tile_load_rows(p, pl, ws, g);
     count_block_balanced(p, pl, ws, g, ntab, a.desc + r, a.faces + (uint64_t)r * a.face_stride);
 }
 
 template <int CPL, bool GENERIC>
 __device__ __forceinline__ void batch_emit_block(const BatchArgs &a, const Problem &p, const WPlan &pl,
-                                                 unsigned char *ws, const uint64_t *tab, const uint8_t *ntab,
-                                                 const uint8_t *owner, uint32_t id, uint32_t r, uint64_t rank_off,
-                                                 const mtx_batch_job_result &jr) {
-    const Geo g = block_geo(id, p, false, 4);
+                                                 const GridDiv &dv, unsigned char *ws, const uint64_t *tab,
+                                                 const uint8_t *ntab, const uint8_t *owner, uint32_t id, uint32_t r,
+                                                 uint64_t rank_off, const mtx_batch_job_result &jr) {
+    const Geo g = block_geo(id, p, false, 4, dv);
     const uint4 q = __ldcg(reinterpret_cast<const uint4 *>(a.desc + r));
     const mtx_meshlet_descriptor d{q.x, q.y, q.z, q.w};
     const uint32_t nb_rk = neighbour_rank<false>(p, g, id, a.rank_pool + rank_off);
@@ -480,8 +482,13 @@ __device__ __forceinline__ void batch_emit_block(const BatchArgs &a, const Probl
 }
 
 // ------------------------------------------------------------ the kernel
-template <int CPL, bool GENERIC>
-__global__ void __launch_bounds__(kBThreads) batch_extract_kernel(const __grid_constant__ BatchArgs a) {
+// BC: every volume's block edge at compile time (0: each volume's own, at run
+// time).  When all volumes of a batch have edge 8 the plan and every division
+// by the edge fold to constants, and the kernel's code gets smaller.  Its
+// register use is held to four CTAs per SM (62 registers, no spills), the
+// occupancy of the run-time-edge variants.
+template <int CPL, bool GENERIC, int BC>
+__global__ void __launch_bounds__(kBThreads, BC ? 4 : 1) batch_extract_kernel(const __grid_constant__ BatchArgs a) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint32_t s_u[4];
     __shared__ uint32_t s_tmp[kBWarps + 1];
@@ -529,8 +536,9 @@ __global__ void __launch_bounds__(kBThreads) batch_extract_kernel(const __grid_c
             const BVol &v = a.vols[job.vol];
             Problem p = v.p;
             p.iso = job.iso;
-            const WPlan pl = v.pl;
-            batch_count_block(a, p, pl, ws, ntab, id, r);
+            if (BC) p.B = BC;
+            const WPlan pl = BC ? make_wplan_balanced(BC) : v.pl;
+            batch_count_block(a, p, pl, v.dv, ws, ntab, id, r);
             ++done;
         }
     }
@@ -572,13 +580,14 @@ __global__ void __launch_bounds__(kBThreads) batch_extract_kernel(const __grid_c
             const BVol &v = a.vols[job.vol];
             Problem p = v.p;
             p.iso = job.iso;
-            const WPlan pl = v.pl;
+            if (BC) p.B = BC;
+            const WPlan pl = BC ? make_wplan_balanced(BC) : v.pl;
             mtx_batch_job_result jr;
             jr.vertexOffset = __ldcg(&a.res[j].vertexOffset);
             jr.indexOffset = __ldcg(&a.res[j].indexOffset);
             jr.vertexCount = __ldcg(&a.res[j].vertexCount);
             jr.indexCount = __ldcg(&a.res[j].indexCount);
-            batch_emit_block<CPL, GENERIC>(a, p, pl, ws, tab, ntab, owner, id, r, job.rank_off, jr);
+            batch_emit_block<CPL, GENERIC>(a, p, pl, v.dv, ws, tab, ntab, owner, id, r, job.rank_off, jr);
         }
     }
 }
@@ -596,7 +605,7 @@ struct mtx_batch {
     uint64_t mm_warps = 0;
     uint32_t grid = 0, smem = 0, vsz = 12;
     uint64_t block_cap = 0, vcap = 0, tcap = 0;
-    int variant = 0;  // CPL 8/32 x GENERIC
+    int variant = 0;  // CPL 8/32 x GENERIC (0-3), edge 8 at compile time x GENERIC (4-5)
     std::vector<void *> allocs;
     BVol *vols = nullptr;
     uint2 *leaf = nullptr;
@@ -614,10 +623,12 @@ namespace {
 using KernelFn = void (*)(BatchArgs);
 KernelFn batch_kernel(int variant) {
     switch (variant) {
-    case 0: return batch_extract_kernel<8, false>;
-    case 1: return batch_extract_kernel<8, true>;
-    case 2: return batch_extract_kernel<32, false>;
-    default: return batch_extract_kernel<32, true>;
+    case 0: return batch_extract_kernel<8, false, 0>;
+    case 1: return batch_extract_kernel<8, true, 0>;
+    case 2: return batch_extract_kernel<32, false, 0>;
+    case 3: return batch_extract_kernel<32, true, 0>;
+    case 4: return batch_extract_kernel<8, false, 8>;
+    default: return batch_extract_kernel<8, true, 8>;
     }
 }
 
@@ -719,6 +730,7 @@ mtx_status mtx_batch_create(mtx_context_t c, const mtx_batch_desc *d, mtx_batch_
         p.GZ = ceil_div(p.Z, B);
         p.nblocks = (uint64_t)p.GX * p.GY * p.GZ;
         bv.pl = plan_in_layout(B, L);
+        bv.dv = grid_div(p);
         bv.vec = ((uintptr_t)p.vol % 16 == 0) && (((uint64_t)p.X * esz) % 16 == 0) && (B == 4 || B == 8 || B == 16);
         bv.leaf_off = leaf_total;
         leaf_total += align4(p.nblocks);
@@ -825,7 +837,9 @@ mtx_status mtx_batch_create(mtx_context_t c, const mtx_batch_desc *d, mtx_batch_
 
     // persistent grid: every CTA that fits at once
     const bool generic = d->vertexFormat != MTX_VERTEX_XYZ || d->frame != MTX_FRAME_VOXEL;
-    b->variant = (Bmax > 8 ? 2 : 0) + (generic ? 1 : 0);
+    bool all8 = true;
+    for (uint32_t v = 0; v < b->nvol; ++v) all8 = all8 && d->blockEdges[v] == 8;
+    b->variant = all8 ? 4 + (generic ? 1 : 0) : (Bmax > 8 ? 2 : 0) + (generic ? 1 : 0);
     // as many block warps per CTA as the shared memory holds (8 unless the
     // largest plan is a 16^3 float32 tile)
     const int static_smem = 1024;

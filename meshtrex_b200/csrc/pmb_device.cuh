@@ -147,7 +147,7 @@ struct GridDiv {
     uint64_t mx, mxy;
     uint32_t dx, dxy;
 };
-__device__ __forceinline__ GridDiv grid_div(const Problem &p) {
+__host__ __device__ inline GridDiv grid_div(const Problem &p) {
     GridDiv d;
     d.dx = p.GX;
     d.dxy = p.GX * p.GY;

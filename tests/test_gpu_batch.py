@@ -107,6 +107,17 @@ def test_batch_vertex_data_ndc_normals(ctx):
     _check_batch(ctx, arrays, blocks, jobs, options=opts, runs=1)
 
 
+@pytest.mark.parametrize("generic", [False, True])
+def test_batch_all_edge_8(ctx, generic):
+    """Every volume at block edge 8: the kernel instantiated with the edge at
+    compile time."""
+    from meshtrex_b200 import _lib as L
+    from meshtrex_b200 import api
+    arrays, _, jobs = _mix(seed=17)
+    opts = api.extract_options(vertex_format=L.VERTEX_DATA, frame=L.FRAME_NDC, normals=True) if generic else None
+    _check_batch(ctx, arrays, [8] * len(arrays), jobs, options=opts, runs=2 - generic)
+
+
 def test_batch_reports_capacity_with_needed_sizes(ctx):
     from meshtrex_b200 import api
     arrays, blocks, jobs = _mix(seed=13)
