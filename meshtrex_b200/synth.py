@@ -9,6 +9,17 @@ The generators are written once in torch so that the same code runs on the
 CPU (tests, CPU baseline) and on the GPU (full-size bench volumes). Parity
 checks always compare the CUDA path and the oracle on the same bytes.
 
+Randomness comes from splitmix64 (Steele, Lea and Flood, "Fast splittable
+pseudorandom number generators", OOPSLA 2014): output i of a stream seeded
+with s is mix(s + (i + 1) * 0x9E3779B97F4A7C15).  Being counter-based, the
+same seed gives the same numbers on the CPU and on the GPU and for any slab
+size.  Scalar draws (blob centres, volume shapes, isovalues) come from
+``Stream``; per-voxel Gaussian noise is Box-Muller over the pair of outputs
+(2i, 2i + 1) of the voxel's flat index i, in float64, then rounded to float32
+(``normal_noise``).  Float32 arithmetic of the fields themselves (exp, sin)
+may still differ in the last bit between the CPU and the GPU, so a check
+copies the bytes it compares rather than regenerating them.
+
 Workloads:
   blobs    256^3 uint8: 8 Gaussian blobs + N(0, 4) noise (std 4), seed 0
   fbm_ball 1024^3 uint16: radial ramp + 0.08 fBm(5 octaves, base freq 4), seed 1
@@ -25,6 +36,73 @@ import numpy as np
 import torch
 
 _M32 = 0xFFFFFFFF
+_M64 = (1 << 64) - 1
+_GOLDEN = 0x9E3779B97F4A7C15
+_MIX1 = 0xBF58476D1CE4E5B9
+_MIX2 = 0x94D049BB133111EB
+_NOISE_KEY = 0x6E6F697365  # xor-ed into a field's seed for its per-voxel noise stream
+
+
+def splitmix64(z: int) -> int:
+    """The splitmix64 output function of a 64-bit state (Python ints)."""
+    z &= _M64
+    z = ((z ^ (z >> 30)) * _MIX1) & _M64
+    z = ((z ^ (z >> 27)) * _MIX2) & _M64
+    return z ^ (z >> 31)
+
+
+def _s64(c: int) -> int:
+    """A 64-bit constant as the int64 with the same bits."""
+    return c - (1 << 64) if c >= 1 << 63 else c
+
+
+def _srl(z: torch.Tensor, s: int) -> torch.Tensor:
+    """Logical right shift of int64 bits."""
+    return (z >> s) & ((1 << (64 - s)) - 1)
+
+
+def _splitmix64_t(z: torch.Tensor) -> torch.Tensor:
+    """splitmix64's output function over an int64 tensor (products wrap mod 2^64)."""
+    z = (z ^ _srl(z, 30)) * _s64(_MIX1)
+    z = (z ^ _srl(z, 27)) * _s64(_MIX2)
+    return z ^ _srl(z, 31)
+
+
+class Stream:
+    """A seeded splitmix64 stream of scalar draws."""
+
+    def __init__(self, seed: int):
+        self.state = seed & _M64
+
+    def next64(self) -> int:
+        self.state = (self.state + _GOLDEN) & _M64
+        return splitmix64(self.state)
+
+    def uniform(self, lo: float = 0.0, hi: float = 1.0, n: int | None = None):
+        """U[lo, hi) from the top 53 bits of one output; a list of n when n is given."""
+        if n is not None:
+            return [self.uniform(lo, hi) for _ in range(n)]
+        return lo + (hi - lo) * ((self.next64() >> 11) * 2.0 ** -53)
+
+    def integer(self, n: int) -> int:
+        """Uniform over 0..n-1."""
+        return min(n - 1, int(self.uniform() * n))
+
+
+def normal_noise(seed: int, first: int, shape, device) -> torch.Tensor:
+    """N(0, 1) float32 noise of the voxels with flat indices first, first + 1, ...
+    (reshaped to `shape`): Box-Muller over outputs 2i and 2i + 1 of the
+    splitmix64 stream seeded with seed ^ 0x6E6F697365."""
+    n = 1
+    for d in shape:
+        n *= int(d)
+    key = _s64(((seed ^ _NOISE_KEY) & _M64))
+    i = torch.arange(first, first + n, device=device, dtype=torch.int64)
+    c1 = key + (2 * i + 1) * _s64(_GOLDEN)
+    u1 = _srl(_splitmix64_t(c1), 11).to(torch.float64) * 2.0 ** -53
+    u2 = _srl(_splitmix64_t(c1 + _s64(_GOLDEN)), 11).to(torch.float64) * 2.0 ** -53
+    z = torch.sqrt(-2.0 * torch.log1p(-u1)) * torch.cos((2.0 * math.pi) * u2)
+    return z.to(torch.float32).view(*shape)
 
 
 def _coords(n: int, device, dtype=torch.float32) -> torch.Tensor:
@@ -103,8 +181,10 @@ class BlobParams:
 
 
 def blob_params(seed: int, n: int = 8) -> BlobParams:
-    r = np.random.default_rng(seed)
-    return BlobParams(r.uniform(0.2, 0.8, (n, 3)), r.uniform(0.05, 0.15, n), r.uniform(0.3, 0.7, n))
+    """n blobs: centres U[0.2, 0.8]^3, then sigmas U[0.05, 0.15], then amplitudes U[0.3, 0.7]."""
+    r = Stream(seed)
+    centres = np.array(r.uniform(0.2, 0.8, 3 * n)).reshape(n, 3)
+    return BlobParams(centres, np.array(r.uniform(0.05, 0.15, n)), np.array(r.uniform(0.3, 0.7, n)))
 
 
 def blob_field(shape_zyx, seed: int, device="cpu", out_dtype=torch.uint8, noise_std=4.0,
@@ -112,7 +192,6 @@ def blob_field(shape_zyx, seed: int, device="cpu", out_dtype=torch.uint8, noise_
     """clamp(round(scale * sum_k A_k exp(-|x-c_k|^2 / (2 s_k^2)) + N(0, noise_std)), dtype range)."""
     Z, Y, X = shape_zyx
     p = blob_params(seed, n_blobs)
-    gen = torch.Generator(device=device).manual_seed(seed)
     out = torch.empty(shape_zyx, dtype=out_dtype, device=device)
     for z0, z1 in _slabs(Z, Y, X):
         x, y, z = _grids(z0, z1, Z, Y, X, device)
@@ -123,7 +202,7 @@ def blob_field(shape_zyx, seed: int, device="cpu", out_dtype=torch.uint8, noise_
             acc += float(p.amps[k]) * torch.exp(-d2 / (2.0 * float(p.sigmas[k]) ** 2))
         acc = acc * scale
         if noise_std:
-            acc += torch.randn(acc.shape, generator=gen, device=device) * noise_std
+            acc += normal_noise(seed, z0 * Y * X, acc.shape, device) * noise_std
         out[z0:z1] = _to_dtype(acc, out_dtype)
     return out
 
@@ -165,14 +244,13 @@ def gyroid(n: int = 2048, seed: int = 2, device="cpu", shape_zyx=None, out=None)
     if out is None:
         out = torch.empty((Z, Y, X), dtype=torch.float32, device=device)
     k = 2.0 * math.pi * 12.0
-    gen = torch.Generator(device=device).manual_seed(seed)
     for z0, z1 in _slabs(Z, Y, X):
         x, y, z = _grids(z0, z1, Z, Y, X, device)
         sx, cx = torch.sin(k * x), torch.cos(k * x)
         sy, cy = torch.sin(k * y), torch.cos(k * y)
         sz, cz = torch.sin(k * z), torch.cos(k * z)
         f = sx * cy + sy * cz + sz * cx
-        f = f + torch.randn(f.shape, generator=gen, device=device) * 0.02
+        f = f + normal_noise(seed, z0 * Y * X, f.shape, device) * 0.02
         out[z0:z1] = f
     return out
 
@@ -204,12 +282,12 @@ class BatchItem:
 
 def batch_specs(seed: int = 3, n: int = 64, edges=EDGES):
     """(shape_zyx, dtype, n_iso) of every volume of the batched workload."""
-    r = np.random.default_rng(seed)
+    r = Stream(seed)
     specs = []
     for _ in range(n):
-        X, Y, Z = (int(e) for e in r.choice(edges, 3))
-        dt = DTYPES[int(r.integers(0, 3))]
-        specs.append(((Z, Y, X), dt, int(r.integers(1, 17))))
+        X, Y, Z = (int(edges[r.integer(len(edges))]) for _ in range(3))
+        dt = DTYPES[r.integer(3)]
+        specs.append(((Z, Y, X), dt, 1 + r.integer(16)))
     return specs
 
 
@@ -217,7 +295,7 @@ def batch(seed: int = 3, n: int = 64, device="cpu", edges=EDGES, scale_down: int
     """64 anisotropic blob volumes of mixed dtypes, each with 1-16 isovalues
     drawn uniformly between its 10th and 90th value percentiles."""
     items = []
-    r = np.random.default_rng(seed + 1000)
+    r = Stream(seed + 1000)
     for i, (shape, dt, n_iso) in enumerate(batch_specs(seed, n, edges)):
         shape = tuple(max(8, s // scale_down) for s in shape)
         scale = {torch.uint8: 255.0, torch.uint16: 65535.0, torch.float32: 1.0}[dt]
