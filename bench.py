@@ -463,7 +463,7 @@ def run_mtx(args):
     if not args.no_batch:
         del exts
         line["batched"] = run_batched(ctx, stream, steps=max(3, min(20, steps)), scale_down=args.batch_scale,
-                                      fixed=args.batch_fixed)
+                                      fixed=args.batch_fixed, with_cpu=not args.no_cpu)
 
     if not args.no_backward:
         line["backward"] = run_backward(ctx, stream, steps=max(3, min(20, steps)))
@@ -583,7 +583,26 @@ def run_e2e(ctx, vol_dev, ws, steps):
                     "step's extractions"}
 
 
-def run_batched(ctx, stream, steps, scale_down=1, fixed=False):
+def batch_cpu_baseline(vols, jobs, blocks, threads: int, target_s: float):
+    """The oracle's full path (min/max, compaction, marching cubes with the mesh
+    written) over the batch's jobs in job order on `threads` host cores, until
+    about target_s: a bounded sample of the workload, in job voxels a second."""
+    from oracle import oracle as O
+    hosts, secs, vox, n = {}, 0.0, 0, 0
+    for v, iso in jobs:
+        if v not in hosts:
+            hosts[v] = vols[v].cpu().numpy()
+        t0 = time.perf_counter()
+        O.extract(hosts[v], blocks[v], iso, nthreads=threads)
+        secs += time.perf_counter() - t0
+        vox += hosts[v].size
+        n += 1
+        if secs >= target_s:
+            break
+    return vox / secs / 1e9, n, secs
+
+
+def run_batched(ctx, stream, steps, scale_down=1, fixed=False, with_cpu=False):
     """The 64-volume mix (anisotropic edges from {64..512}, uint8/uint16/float32,
     1-16 isovalues each, seed 3): one batched run per step (a CUDA graph of the
     batched min/max and the persistent extraction kernel) against the same
@@ -715,6 +734,14 @@ def run_batched(ctx, stream, steps, scale_down=1, fixed=False):
     for e in exts:
         del e
     b.close()
+    if with_cpu:
+        threads = nproc()
+        g_all, n_all, s_all = batch_cpu_baseline(vols, jobs, blocks, threads, 10.0)
+        g_one, n_one, s_one = batch_cpu_baseline(vols, jobs, blocks, 1, 10.0)
+        out["cpu_baseline"] = {
+            "allcore_gvoxels_per_s": g_all, "1thread_gvoxels_per_s": g_one, "cores": threads, "kind": "port",
+            "sample": (f"the first {n_all} jobs in job order on all threads ({s_all:.1f} s) and the first {n_one} "
+                       f"on one thread ({s_one:.1f} s), each job's full mesh at its block edge")}
     return out
 
 
