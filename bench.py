@@ -284,13 +284,21 @@ def run_reference(args):
 
 
 # --------------------------------------------------------------- GPU side
-def launches_per_extraction(grid):
+def launches_per_extraction(grid, shape_zyx=None, esz=2, block=BLOCK):
+    """Kernel launches of one plain extraction: leaf min/max (with the strip-column
+    patch when the TMA leaf pass covers more than one 512-byte x-strip), octree,
+    filter, count + scan, emit."""
     m = max(grid)
     levels = 1
     while m > 1:
         m >>= 1
         levels += 1
-    return 1 + (1 if levels > 1 else 0) + 1 + 2 + 1  # leaf, octree, filter, count + scan, emit
+    patch = 0
+    if shape_zyx is not None:
+        X = shape_zyx[2]
+        tma_leaf = esz >= 2 and (X * esz) % 16 == 0 and block in (4, 8, 16)
+        patch = 1 if tma_leaf and X * esz > 512 else 0
+    return 1 + patch + (1 if levels > 1 else 0) + 1 + 2 + 1
 
 
 def read_traffic():
@@ -445,7 +453,7 @@ def run_mtx(args):
             "pipeline_roofline": {"achieved": pipe_gbs, "peak": peak, "unit": "GB/s", "frac": pipe_gbs / peak,
                                   "bytes_per_step": step_bytes,
                                   "what": "volume read once per extraction + mesh written (12 B/vertex, 12 B/triangle)"},
-            "gpu_launches": launches_per_extraction(grid) * 3 * steps,
+            "gpu_launches": launches_per_extraction(grid, (N, N, N), 2, BLOCK) * 3 * steps,
             "clocks": clk}
 
     if rank == 0 and not args.no_cpu:
@@ -724,7 +732,8 @@ def run_batched(ctx, stream, steps, scale_down=1, fixed=False, with_cpu=False):
                      "peak_kind": peak_kind},
         "gpu_launches_per_step": 2,
         "plain_launches_per_step": sum(launches_per_extraction(tuple((n + blocks[v] - 1) // blocks[v]
-                                                                     for n in vols[v].shape)) for v, _ in jobs),
+                                                                     for n in vols[v].shape), tuple(vols[v].shape),
+                                                               vols[v].element_size(), blocks[v]) for v, _ in jobs),
         "autotuned": {"block_edges": sorted(set(blocks)), "block_edge_per_dtype": {
             str(dt).replace("torch.", ""): sorted({blocks[v] for v in range(len(vols)) if vols[v].dtype == dt})
             for dt in (torch.uint8, torch.uint16, torch.float32)}, "block_warps": block_warps,

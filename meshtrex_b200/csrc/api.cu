@@ -451,7 +451,7 @@ mtx_status mtx_context_destroy(mtx_context_t c) {
     join_extract(c);
     cudaStreamSynchronize(c->stream);
     for (Scratch *s : {&c->filter_status, &c->count_status, &c->faces, &c->state, &c->leaf, &c->ids, &c->rank,
-                       &c->desc, &c->misc, &c->adj_partial, &c->adj_iso})
+                       &c->desc, &c->misc, &c->adj_partial, &c->adj_iso, &c->xface})
         dev_free(c, s->ptr);
     dev_cache_release(c->device);
     if (c->copy_stream) cudaStreamDestroy(c->copy_stream);

@@ -28,20 +28,24 @@ __global__ void __launch_bounds__(128) minmax_leaf_vec_kernel(const T *__restric
 // four per SM.  A work item is (x-strip of 512 bytes, run of ZC block slabs,
 // group of four block rows), taken in that order so that the strips of one row
 // and the items sharing a halo slice or row run side by side (L2 serves the
-// repeats, DRAM sees whole rows).  Per z
-// slice thread 0 issues two TMA boxes into a ring of S stages: the strip's
-// 4B+1 rows and, beyond them, the 16-byte halo column (out-of-volume parts
-// read as zero and are masked).  Warp w folds block row w of the group with
-// the per-lane arithmetic of the load-based body: lane l owns 16 bytes of
-// every row, the +1 column of a block comes from the next lane by shuffle
-// (lane 31: from the halo box), and a slice at z = (bz+1)*B closes block bz
-// and opens bz+1; rows fold two at a time with three-input packed min/max.
-// Loads in flight live in shared memory (about 35 KB per CTA), not in
+// repeats, DRAM sees whole rows).  Per z slice thread 0 issues one TMA box of
+// the strip's 4B+1 rows into a ring of S stages (out-of-volume parts read as
+// zero and are masked).  Warp w folds block row w of the group with the
+// per-lane arithmetic of the load-based body: lane l owns 16 bytes of every
+// row, the +1 column of a block comes from the next lane by shuffle, and a
+// slice at z = (bz+1)*B closes block bz and opens bz+1; rows fold two at a
+// time with three-input packed min/max.
+// The +1 column of a strip's last block is the next strip's first column.
+// Loaded beside the strip, that 16-byte column cost a 32-byte DRAM sector
+// per row (98 MB, 4.6% of a 1024^3 uint16 volume, 0.016 ms of 0.353): instead
+// lane 0 of every strip but the first folds its own first column over each
+// block's (B+1)^2 rows and slices into xface, and minmax_xface_patch_kernel
+// merges it into the previous strip's last block (and its level-1 texel).
+// Loads in flight live in shared memory (about 34 KB per CTA), not in
 // registers, so an SM keeps room for the extraction kernels of other streams.
 constexpr int kTmaRows(int B) { return 4 * B + 1; }
 constexpr uint32_t kTmaMain(int B) { return (uint32_t)kTmaRows(B) * 512u; }
-constexpr uint32_t kTmaHalo(int B) { return ((uint32_t)kTmaRows(B) * 16u + 127u) / 128u * 128u; }
-constexpr uint32_t kTmaStage(int B) { return (kTmaMain(B) + 127u) / 128u * 128u + kTmaHalo(B); }
+constexpr uint32_t kTmaStage(int B) { return (kTmaMain(B) + 127u) / 128u * 128u; }
 constexpr int kTmaStages(int B) { return B == 4 ? 4 : 2; }  // about 35 KB per CTA at B = 4 and 8
 constexpr int kTmaCtasPerSm = 4;  // 16 warps: enough to hide the fold's latencies, smem left for other kernels
 
@@ -57,11 +61,12 @@ struct TmaLeafArgs {
 // warp's z run, the x pair by shuffle, the y pair (warps w and w + 1) through
 // shared memory after the slice's barrier.  Blocks outside the grid count as
 // the identity {~0, 0}.
+// xface: (nXS - 1) x GY x GZ strip-start columns (minmax_xface_patch_kernel).
 template <typename T, int B>
 __global__ void __launch_bounds__(128) minmax_leaf_tma_kernel(const __grid_constant__ CUtensorMap map_main,
-                                                                 const __grid_constant__ CUtensorMap map_halo,
                                                                  const TmaLeafArgs a, uint2 *__restrict__ leaf,
-                                                                 uint2 *__restrict__ l1, DevStatus *st) {
+                                                                 uint2 *__restrict__ l1, uint2 *__restrict__ xface,
+                                                                 DevStatus *st) {
     using L16 = Lane16<T>;
     constexpr int V = L16::V;
     constexpr int SEG = 32 * V;
@@ -70,8 +75,7 @@ __global__ void __launch_bounds__(128) minmax_leaf_tma_kernel(const __grid_const
     constexpr int CNT = V >= B ? B : V;      // elements of one block in one lane
     constexpr int S = kTmaStages(B);
     constexpr uint32_t MAIN = kTmaMain(B), STAGE = kTmaStage(B);
-    constexpr uint32_t HOFF = (MAIN + 127u) / 128u * 128u;
-    constexpr uint32_t TX = MAIN + (uint32_t)kTmaRows(B) * 16u;  // bytes per stage
+    constexpr uint32_t TX = MAIN;  // bytes per stage
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t bars[S];
     __shared__ uint32_t s_fail;
@@ -83,7 +87,6 @@ __global__ void __launch_bounds__(128) minmax_leaf_tma_kernel(const __grid_const
         fence_mbar_init();
         s_fail = 0;
         prefetch_tensormap(&map_main);
-        prefetch_tensormap(&map_halo);
     }
     __syncthreads();
 
@@ -114,7 +117,6 @@ __global__ void __launch_bounds__(128) minmax_leaf_tma_kernel(const __grid_const
         mbar_arrive_expect_tx(bar, TX);
         const int x0 = (int)(pxs * SEG), y0 = (int)(pg * 4 * B);
         tma_load_3d(dst, &map_main, bar, x0, y0, (int)pz);
-        tma_load_3d(dst + HOFF, &map_halo, bar, x0 + SEG, y0, (int)pz);
         ++issued;
         if (++pz > pze) {
             pk += gridDim.x;
@@ -134,9 +136,16 @@ __global__ void __launch_bounds__(128) minmax_leaf_tma_kernel(const __grid_const
         item_of(k, xs, g, zs, ze, bz0, bz1);
         const uint32_t x0 = xs * SEG + lane * V;
         const bool on = x0 < a.X;  // X is a multiple of V
-        const bool halo_on = lane == 31 && xs * SEG + SEG < a.X;
         const uint32_t by = g * 4 + w;
         const bool row_on = by < a.GY;
+        // lane 0 of a strip that has one to its left: the first column, per block
+        const bool f_on = lane == 0 && xs > 0 && row_on && on;
+        uint32_t fmn = ~0u, fmx = 0u;
+        auto f_write = [&](uint32_t cbz) {
+            if (f_on && MTX_BC(((uint64_t)cbz * a.GY + by) * (a.nXS - 1) + xs - 1,
+                               (uint64_t)(a.nXS - 1) * a.GY * a.GZ, kBcLeaf))
+                xface[((uint64_t)cbz * a.GY + by) * (a.nXS - 1) + xs - 1] = make_uint2(fmn, fmx);
+        };
         const uint32_t ny = row_on ? min((uint32_t)B + 1u, a.Y - by * B) : 0u;
         uint32_t amn[NB], amx[NB];
 #pragma unroll
@@ -186,7 +195,6 @@ __global__ void __launch_bounds__(128) minmax_leaf_tma_kernel(const __grid_const
             // row 0, then two rows per three-input min/max; rows past the volume
             // read row 0 again, which leaves min and max unchanged
             uint4 mn = L16::lo_id(), mx = L16::hi_id();
-            uint32_t hmn = ~0u, hmx = 0u;
             if (on) {
                 const unsigned char *src = stg + w * B * 512u + lane * 16u;
                 auto row = [&](int r) {
@@ -197,20 +205,14 @@ __global__ void __launch_bounds__(128) minmax_leaf_tma_kernel(const __grid_const
                 for (int r = 1; r + 1 <= B; r += 2) L16::fold2(mn, mx, row(r), row(r + 1));
                 if constexpr (B % 2 == 1) L16::fold2(mn, mx, row(B), row(B));
             }
-            if (halo_on) {
-#pragma unroll
-                for (int r = 0; r <= B; ++r) {
-                    if ((uint32_t)r < ny) {
-                        const uint32_t hk = Vox<T>::key(*reinterpret_cast<const T *>(stg + HOFF + (w * B + r) * 16u));
-                        hmn = min(hmn, hk);
-                        hmx = max(hmx, hk);
-                    }
-                }
-            }
-            // first column of the next lane is this lane's halo column
-            uint32_t nmn = __shfl_down_sync(0xffffffffu, L16::elem(mn, 0, false), 1);
-            uint32_t nmx = __shfl_down_sync(0xffffffffu, L16::elem(mx, 0, true), 1);
-            if (lane == 31) { nmn = hmn; nmx = hmx; }
+            // first column of the next lane is this lane's halo column; lane 31's
+            // is the next strip's first column, merged in by the patch kernel
+            const uint32_t c0mn = L16::elem(mn, 0, false), c0mx = L16::elem(mx, 0, true);
+            uint32_t nmn = __shfl_down_sync(0xffffffffu, c0mn, 1);
+            uint32_t nmx = __shfl_down_sync(0xffffffffu, c0mx, 1);
+            if (lane == 31) { nmn = ~0u; nmx = 0u; }
+            fmn = min(fmn, c0mn);
+            fmx = max(fmx, c0mx);
             uint32_t smn[NB], smx[NB];
 #pragma unroll
             for (int j = 0; j < NB; ++j) {
@@ -262,6 +264,9 @@ __global__ void __launch_bounds__(128) minmax_leaf_tma_kernel(const __grid_const
                     chi = hi;
                 }
                 if (l1) l1_close(clo, chi, bz);
+                f_write(bz);
+                fmn = c0mn;  // the closing slice opens the next block
+                fmx = c0mx;
                 ++bz;
             }
             __syncthreads();  // every warp is done with this stage
@@ -289,6 +294,7 @@ __global__ void __launch_bounds__(128) minmax_leaf_tma_kernel(const __grid_const
                 clo = lo;
                 chi = hi;
             }
+            f_write(bz);
             if (l1) {
                 l1_close(clo, chi, bz);
                 __syncthreads();
@@ -299,6 +305,36 @@ __global__ void __launch_bounds__(128) minmax_leaf_tma_kernel(const __grid_const
     // no copy may still be in flight into this CTA's shared memory when it exits
     if (tid == 0)
         for (; seq < issued; ++seq) mbar_wait_bounded(&bars[seq % S], (seq / S) & 1u);
+}
+
+// Merges each strip-start column record (the x halo the TMA leaf pass leaves
+// out) into the last block of the strip before it: the leaf entry, and, when
+// the leaf pass wrote octree level 1, the texel that holds that block.  One
+// record per leaf entry; four records share a texel, hence the atomics there.
+__global__ void __launch_bounds__(256) minmax_xface_patch_kernel(uint2 *__restrict__ leaf, uint2 *__restrict__ l1,
+                                                                 const uint2 *__restrict__ xface, uint32_t GX,
+                                                                 uint32_t GY, uint32_t GZ, uint32_t nS, uint32_t SB,
+                                                                 uint32_t E1x, uint32_t E1y, uint32_t E1z) {
+    const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (uint64_t)nS * GY * GZ) return;
+    const uint32_t s = (uint32_t)(e % nS);
+    const uint64_t rest = e / nS;
+    const uint32_t by = (uint32_t)(rest % GY), bz = (uint32_t)(rest / GY);
+    const uint32_t bx = (s + 1) * SB - 1;
+    const uint2 f = xface[e];
+    const uint64_t li = ((uint64_t)bz * GY + by) * GX + bx;
+    if (bx < GX && MTX_BC(li, (uint64_t)GX * GY * GZ, kBcLeaf)) {
+        const uint2 v = leaf[li];
+        leaf[li] = make_uint2(min(v.x, f.x), max(v.y, f.y));
+    }
+    if (l1) {
+        const uint32_t X1 = bx >> 1, Y1 = by >> 1, Z1 = bz >> 1;
+        if (X1 < E1x && Y1 < E1y && Z1 < E1z) {
+            uint2 *t = l1 + ((uint64_t)Z1 * E1y + Y1) * E1x + X1;
+            atomicMin(&t->x, f.x);
+            atomicMax(&t->y, f.y);
+        }
+    }
 }
 
 // Fallback for any block edge and any row alignment: one thread per block.
@@ -430,9 +466,8 @@ template <typename T, int B>
 static mtx_status launch_tma(mtx_context *c, const Problem &p, uint2 *leaf, cudaStream_t s, uint32_t zover,
                              uint2 *l1, const uint32_t *l1ext, bool *l1_done) {
     constexpr uint32_t SEG = 32 * (16 / sizeof(T));
-    CUtensorMap mmain, mhalo;
+    CUtensorMap mmain;
     mtx_status r = make_volume_tensor_map_box(c, p, SEG, kTmaRows(B), 1, &mmain);
-    if (r == MTX_OK) r = make_volume_tensor_map_box(c, p, 16 / sizeof(T), kTmaRows(B), 1, &mhalo);
     if (r != MTX_OK) return r;
     TmaLeafArgs a;
     a.X = p.X; a.Y = p.Y; a.Z = p.Z;
@@ -464,10 +499,19 @@ static mtx_status launch_tma(mtx_context *c, const Problem &p, uint2 *leaf, cuda
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, 128, smem);
     if (e != cudaSuccess) return cuda_fail(c, e, "minmax tma occupancy");
     occ = std::max(1, std::min(occ, kTmaCtasPerSm));
+    const uint64_t nface = (uint64_t)(a.nXS - 1) * a.GY * a.GZ;  // strip-start column records
+    if (nface && (r = scratch_reserve(c, c->xface, nface * sizeof(uint2))) != MTX_OK) return r;
+    uint2 *xface = nface ? (uint2 *)c->xface.ptr : nullptr;
     const uint32_t grid = std::min<uint32_t>(a.nitems, (uint32_t)c->sm_count * (uint32_t)occ);
-    k<<<grid, 128, smem, s>>>(mmain, mhalo, a, leaf, with_l1 ? l1 : nullptr, &c->ctrl->status);
+    k<<<grid, 128, smem, s>>>(mmain, a, leaf, with_l1 ? l1 : nullptr, xface, &c->ctrl->status);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(c, e, "minmax tma launch");
+    if (nface) {
+        minmax_xface_patch_kernel<<<(unsigned)((nface + 255) / 256), 256, 0, s>>>(
+            leaf, with_l1 ? l1 : nullptr, xface, a.GX, a.GY, a.GZ, a.nXS - 1, SEG / B, a.E1[0], a.E1[1], a.E1[2]);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(c, e, "minmax halo patch launch");
+    }
     return MTX_OK;
 }
 

@@ -47,6 +47,7 @@ struct mtx_context {
     mtx::Ctrl *ctrl = nullptr;   // device
     uint32_t *pinned = nullptr;  // pinned host words for count readbacks
     mtx::Scratch filter_status, count_status, faces, state, leaf, ids, rank, desc, misc;
+    mtx::Scratch xface;  // leaf pass: the first column of every x-strip but the first, per block row and slab
     mtx::Scratch adj_partial, adj_iso;  // adjoint: per-block partial tiles and isovalue sums
     mtx_profiler *prof = nullptr;  // records stage times of calls given no profiler
     mtx_tuning tuning = {0, 0, 0, 0, 0};
