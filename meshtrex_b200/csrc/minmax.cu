@@ -3,9 +3,9 @@
 // minMaxOctreeReduce.comp.glsl:23-59, dispatched by minMaxPass.cpp:147-253).
 //
 // The leaf pass streams the volume once from HBM (the warp layout is described
-// in minmax_device.cuh).  Only the halo row of the y direction is read twice,
-// by two warps that run side by side, so DRAM sees each voxel once and L2
-// serves the repeat.
+// in minmax_device.cuh).  The halo rows and slices it reads twice are read by
+// items that run side by side, so L2 serves the repeat; the TMA pass reads no
+// halo column at all (minmax_xface_patch_kernel).
 #include <algorithm>
 #include <cstring>
 
