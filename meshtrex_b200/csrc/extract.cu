@@ -28,9 +28,10 @@ constexpr bool kSingleBuffer = true;
 // ------------------------------------------------------------- count pass
 // BC: the block edge at compile time (0: p.B at run time).  The bench's edge 8
 // has its own instantiation, in which the warp's shared-memory plan and every
-// division by the edge fold to constants.
+// division by the edge fold to constants (40 registers).  The run-time form is
+// held to 64 registers (no spills), where it would otherwise take up to 128.
 template <typename T, bool TMA, int BC>
-__global__ void __launch_bounds__(kMaxWarps * 32)
+__global__ void __launch_bounds__(kMaxWarps * 32, BC ? 0 : 4)
     pmb_count_kernel(Problem p_, const __grid_constant__ CUtensorMap map, const uint32_t *__restrict__ ids,
                      const uint32_t *__restrict__ count_ptr, mtx_meshlet_descriptor *__restrict__ desc,
                      uint64_t desc_cap, uint32_t *__restrict__ faces, uint8_t *__restrict__ state,
@@ -81,12 +82,14 @@ __global__ void __launch_bounds__(kMaxWarps * 32)
             if (have_next && pl.nbuf == 2) tile_drain<TMA>(pl, ws, buf ^ 1u, parity);
             break;
         }
-        count_block<T>(p, pl, ws, buf, g, ntab, cell_cases ? cell_cases + (uint64_t)r * B3 : nullptr, desc + r,
-                       faces + (uint64_t)r * 3 * pl.BB,
-                       (state && pl.state_bytes) ? state + (uint64_t)r * pl.state_bytes : nullptr);
+        // one tile buffer: the next tile is issued as soon as this block's rows are built
+        const bool early = have_next && pl.nbuf == 1;
+        count_block<T, TMA>(p, pl, ws, buf, g, ntab, cell_cases ? cell_cases + (uint64_t)r * B3 : nullptr, desc + r,
+                            faces + (uint64_t)r * 3 * pl.BB,
+                            (state && pl.state_bytes) ? state + (uint64_t)r * pl.state_bytes : nullptr,
+                            early ? &gn : nullptr, &map);
         if (!have_next) break;
-        if (pl.nbuf == 1) tile_issue<T, TMA>(pl, ws, buf, gn, &map);
-        else buf ^= 1u;
+        if (pl.nbuf != 1) buf ^= 1u;
         r = rn;
         g = gn;
     }

@@ -990,13 +990,17 @@ __device__ __forceinline__ void write_face_records(const WPlan &pl, const unsign
 // Count body of one block whose tile is staged: the (vertices, triangles)
 // counts into *dr and the low-face records -- block-relative prefix | mask
 // << 24 of the voxels with x == 0 (index z*B+y), y == 0 (BB + z*B+x) and
-// z == 0 (2BB + y*B+x) -- into fr.
-template <typename T>
+// z == 0 (2BB + y*B+x) -- into fr.  The tile is dead once the inside rows
+// are built: next (TMA, one tile buffer) is then issued into the same buffer,
+// so that its load runs under the rest of this block.
+template <typename T, bool TMA = false>
 __device__ __forceinline__ void count_block(const Problem &p, const WPlan &pl, unsigned char *ws, uint32_t buf,
                                             const Geo &g, const uint8_t *ntab, uint8_t *cases_out,
-                                            mtx_meshlet_descriptor *dr, uint32_t *fr, uint8_t *state) {
+                                            mtx_meshlet_descriptor *dr, uint32_t *fr, uint8_t *state,
+                                            const Geo *next = nullptr, const CUtensorMap *map = nullptr) {
     const uint32_t lane = threadIdx.x & 31;
     build_rows<T>(p, pl, ws, buf, g);
+    if (next) tile_issue<T, TMA>(pl, ws, buf, *next, map);
     uint32_t bnv, bnt;
     block_counts(p, pl, ws, g, ntab, true, cases_out, bnv, bnt, state != nullptr);
     if (lane == 0) *reinterpret_cast<uint2 *>(&dr->vertexCount) = make_uint2(bnv, bnt);

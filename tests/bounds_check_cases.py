@@ -31,7 +31,9 @@ def main():
     ctx = api.Context(0)
     cases = [((32, 32, 32), np.uint8, 8, "tma"), ((37, 29, 41), np.uint8, 4, "ldg"), ((48, 40, 64), np.uint16, 8, "tma"),
              ((33, 31, 30), np.uint16, 3, "ldg"), ((40, 36, 32), np.float32, 8, "tma"),
-             ((50, 47, 64), np.uint16, 16, "tma"), ((21, 19, 32), np.uint8, 2, "ldg"), ((17, 16, 16), np.float32, 8, "ldg")]
+             ((50, 47, 64), np.uint16, 16, "tma"), ((21, 19, 32), np.uint8, 2, "ldg"), ((17, 16, 16), np.float32, 8, "ldg"),
+             # several x-strips of the leaf pass: strip-start column records and their patch
+             ((24, 20, 600), np.uint16, 8, "tma"), ((20, 18, 300), np.float32, 4, "tma")]
     for shape, dt, B, staging in cases:
         a = blob_volume(shape, dt, seed=sum(shape) + B)
         iso = mid_iso(a)
