@@ -91,9 +91,9 @@ __host__ __device__ inline WPlan make_wplan(uint32_t B, uint32_t esz, bool tma, 
     // the emit pass puts its vertex table (build_utab, B <= 8) in the tile's slot
     const uint32_t slot = (tri_pass && B <= 8) ? std::max(p.tile_bytes, 3 * p.B1 * p.B1 * p.B1) : p.tile_bytes;
     uint32_t o = 0;
-    for (uint32_t b = 0; b < 2; ++b) {
+    for (uint32_t b = 0; b < 2; ++b) {  // a TMA destination is 128-byte aligned; what follows the last, 16
         p.off_tile[b] = o;
-        if (b < p.nbuf) o = align_up(o + slot, 128);
+        if (b < p.nbuf) o = align_up(o + slot, b + 1 < p.nbuf ? 128 : 16);
     }
     if (p.nbuf == 1) p.off_tile[1] = p.off_tile[0];
     p.off_bar = o;
@@ -115,9 +115,9 @@ __host__ __device__ inline WPlan make_wplan(uint32_t B, uint32_t esz, bool tma, 
         o = align_up(o + 2 * B * B, 16);
         p.state_bytes = B <= 8 ? o - p.off_cross : 0u;
     }
-    if (tri_pass) {
+    if (tri_pass) {  // context first vertices: 16-bit packed entries for B <= 8 (gather_finish<CPL, true>)
         p.off_nvid = o;
-        o = align_up(o + 4 * p.nb3, 16);
+        o = align_up(o + (B <= 8 ? 2 : 4) * p.nb3, 16);
         p.off_nm = o;
         o = align_up(o + p.nb3, 16);
     }
@@ -743,13 +743,13 @@ __device__ __forceinline__ void build_utab(const WPlan &pl, unsigned char *ws, u
             run += __popc(m);
         }
     }
-    const uint32_t *nvid = reinterpret_cast<const uint32_t *>(ws + pl.off_nvid);
+    const uint16_t *nvid = reinterpret_cast<const uint16_t *>(ws + pl.off_nvid);
     const uint8_t *nm = ws + pl.off_nm;
     for (uint32_t j = lane; j < pl.nb3; j += 32) {
         const uint32_t e = cmap[j];
         const uint32_t ti = (((e >> 23) & 31u) * B1 + ((e >> 18) & 31u)) * B1 + ((e >> 13) & 31u);
         if (MTX_BC(ti, B1 * B1 * B1, kBcVoxTab)) {
-            ut[ti] = (uint16_t)nvid[j];
+            ut[ti] = nvid[j];
             um[ti] = nm[j];
         }
     }
@@ -941,6 +941,7 @@ __device__ __forceinline__ void gather_finish(const WPlan &pl, uint32_t nb_vb, c
                                               unsigned char *ws, uint32_t vbase = 0) {
     const uint32_t lane = threadIdx.x & 31, nb3 = pl.nb3;
     uint32_t *nvid = reinterpret_cast<uint32_t *>(ws + pl.off_nvid);
+    uint16_t *nvid16 = reinterpret_cast<uint16_t *>(ws + pl.off_nvid);
     uint8_t *nm = ws + pl.off_nm;
     if constexpr (PACKED) {
         if (lane < 8) reinterpret_cast<uint32_t *>(ws + pl.off_bar + 16)[lane] = lane ? nb_vb : vbase;
@@ -953,7 +954,7 @@ __device__ __forceinline__ void gather_finish(const WPlan &pl, uint32_t nb_vb, c
         if (j < nb3) {
             const bool present = rec[k] >> 31;
             if constexpr (PACKED)
-                nvid[j] = (rec[k] & 0x7ffu) | (((rec[k] >> 27) & 7u) << 11);
+                nvid16[j] = (uint16_t)((rec[k] & 0x7ffu) | (((rec[k] >> 27) & 7u) << 11));
             else
                 nvid[j] = present ? vb + (rec[k] & 0xffffffu) : kNoVertex;
             nm[j] = present ? (uint8_t)((rec[k] >> 24) & 7u) : (uint8_t)0;
