@@ -26,6 +26,10 @@ CASES = [
     ((72, 40, 264), np.uint16, 8, 2),    # level 1 in the pass: grid 33 x 5 x 9, the last slab unpaired
     ((56, 24, 136), np.float32, 8, 4),   # level 1, two lanes a block: grid 17 x 3 x 7
     ((40, 40, 264), np.uint16, 16, 2),   # level 1, block 16: grid 17 x 3 x 3
+    # strip-start column records merged into the previous strip's last block (and its level-1 texel)
+    ((24, 20, 600), np.uint16, 4, 0),    # two blocks a lane, three strips, the last one partial
+    ((40, 24, 384), np.float32, 4, 2),   # level 1, one block a lane: three full strips of 128 voxels
+    ((34, 41, 1024), np.uint16, 8, 0),   # four full strips: the 1024-voxel rows of the bench volume
 ]
 
 
