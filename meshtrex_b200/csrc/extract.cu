@@ -143,6 +143,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32, (!GENERIC && CPL == 8) ? 3 : 1
     }
     for (uint32_t j = threadIdx.x; j < pl.nb3; j += blockDim.x) cmap[j] = ctx_map_entry(pl, j);
     if (threadIdx.x < 12) owner[threadIdx.x] = c_mc_owner[threadIdx.x];
+    if (CPL == 8) edge_offsets(reinterpret_cast<uint16_t *>(owner + 16), pl.B1);
     if (lane == 0 && TMA) {
         uint64_t *bar = reinterpret_cast<uint64_t *>(ws + pl.off_bar);
         mbar_init(bar, 1);

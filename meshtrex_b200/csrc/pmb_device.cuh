@@ -31,10 +31,11 @@ static mtx_status load_case_tables(mtx_context *c) {
 }
 
 constexpr uint32_t kNoVertex = 0xffffffffu;
-// packed cases (2048 B), triangle counts (256 B), owners (16 B), rounded up so
-// that every warp's region -- and the TMA tile at its start -- is 128-byte aligned
+// packed cases (2048 B), triangle counts (256 B), owners (16 B), the emit
+// pass's edge offsets (24 B, edge_offsets), rounded up so that every warp's
+// region -- and the TMA tile at its start -- is 128-byte aligned
 constexpr uint32_t kTableBytes = 2432;
-static_assert(kTableBytes % 128 == 0 && kTableBytes >= 2048 + 256 + 16, "table region must keep warp regions aligned");
+static_assert(kTableBytes % 128 == 0 && kTableBytes >= 2048 + 256 + 16 + 24, "table region must keep warp regions aligned");
 constexpr uint32_t kJobWin = 256;                   // jobs (vertices or triangles) resolved per window
 constexpr int kMaxWarps = 8;                        // warps per CTA of the extraction kernels
 
@@ -756,12 +757,22 @@ __device__ __forceinline__ void build_utab(const WPlan &pl, unsigned char *ws, u
     __syncwarp();
 }
 
+// Edge offsets of the unified table for one CTA (B <= 8): entry e holds the
+// table offset of cube edge e's owner voxel from the cell's low corner,
+// dx + dy (B+1) + dz (B+1)^2, and its axis << 8 (from the owner table).
+__device__ __forceinline__ void edge_offsets(uint16_t *eoff, uint32_t B1) {
+    if (threadIdx.x < 12) {
+        const uint32_t o = c_mc_owner[threadIdx.x];
+        eoff[threadIdx.x] = (uint16_t)((o & 1u) + ((o >> 1) & 1u) * B1 + ((o >> 2) & 1u) * B1 * B1 + ((o >> 3) << 8));
+    }
+}
+
 // The vertex id of cube edge e of the cell whose low corner is tile voxel ti,
 // from the unified table (build_utab); nbase: the eight block first vertices.
-__device__ __forceinline__ uint32_t edge_vertex_ut(uint32_t ti, uint32_t e, const uint8_t *owner, const uint16_t *ut,
+__device__ __forceinline__ uint32_t edge_vertex_ut(uint32_t ti, uint32_t e, const uint16_t *eoff, const uint16_t *ut,
                                                    const uint8_t *um, const uint32_t *nbase, uint32_t B1, bool &bad) {
-    const uint32_t o = owner[e];
-    const uint32_t i = ti + (o & 1u) + ((o >> 1) & 1u) * B1 + ((o >> 2) & 1u) * B1 * B1, ax = o >> 3;
+    const uint32_t eo = eoff[e];
+    const uint32_t i = ti + (eo & 0xffu), ax = eo >> 8;
     if (!MTX_BC(i, B1 * B1 * B1, kBcVoxTab)) {
         bad = true;
         return 0;
@@ -1109,9 +1120,10 @@ __device__ __forceinline__ void emit_block(const Problem &p, const WPlan &pl, un
                 uint32_t *o = indices + 3ull * (tbase + w0 + b + lane);  // each lane its own 12 bytes
                 if constexpr (VT) {
                     const uint32_t ti = (z * pl.B1 + y) * pl.B1 + x;
-                    o[0] = edge_vertex_ut(ti, (uint32_t)(w & 0xFu), owner, vt, um, nbase, pl.B1, bad);
-                    o[1] = edge_vertex_ut(ti, (uint32_t)((w >> 4) & 0xFu), owner, vt, um, nbase, pl.B1, bad);
-                    o[2] = edge_vertex_ut(ti, (uint32_t)((w >> 8) & 0xFu), owner, vt, um, nbase, pl.B1, bad);
+                    const uint16_t *eoff = reinterpret_cast<const uint16_t *>(owner + 16);  // edge_offsets
+                    o[0] = edge_vertex_ut(ti, (uint32_t)(w & 0xFu), eoff, vt, um, nbase, pl.B1, bad);
+                    o[1] = edge_vertex_ut(ti, (uint32_t)((w >> 4) & 0xFu), eoff, vt, um, nbase, pl.B1, bad);
+                    o[2] = edge_vertex_ut(ti, (uint32_t)((w >> 8) & 0xFu), eoff, vt, um, nbase, pl.B1, bad);
                 } else {
                     o[0] = edge_vertex(x, y, z, (uint32_t)(w & 0xFu), owner, cross, vp, nvid, nm, B, BB,
                                        d.vertexOffset, bad);
