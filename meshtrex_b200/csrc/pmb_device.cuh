@@ -1062,7 +1062,9 @@ __device__ __forceinline__ void emit_block(const Problem &p, const WPlan &pl, un
     // triangles in canonical order: each lane walks the mixed cells of its rows
     // (masks and case bytes kept by block_counts) and writes one job per
     // triangle (cell | t << 12 | case << 16) at the triangle's own position in
-    // a window of kJobWin jobs; the warp resolves 32 triangles at a time
+    // a window of kJobWin jobs; the warp resolves 32 triangles at a time.  With
+    // the vertex table (VT) the cell is given by its low corner's table index
+    // (z (B+1) + y) (B+1) + x, which the resolve uses as is.
     const uint16_t *mmk = reinterpret_cast<const uint16_t *>(ws + pl.off_mm);
     const uint8_t *ck = ws + pl.off_case;
     uint16_t *vt = reinterpret_cast<uint16_t *>(ws + pl.off_tile[buf]);  // the tile is dead past the vertices
@@ -1078,11 +1080,12 @@ __device__ __forceinline__ void emit_block(const Problem &p, const WPlan &pl, un
                 const uint32_t q = lane * R + k;
                 if (q >= BB) break;
                 uint32_t j = tp[q], mm = mmk[q];
+                const uint32_t cell0 = VT ? (q + fdiv(q, pl.rB)) * pl.B1 : q * B;  // row q = z B + y
                 while (mm) {
                     const uint32_t x = __ffs(mm) - 1;
                     mm &= mm - 1u;
                     const uint32_t cfg = ck[q * B + x];
-                    const uint32_t n = ntab[cfg], job = (q * B + x) | (cfg << 16);
+                    const uint32_t n = ntab[cfg], job = (cell0 + x) | (cfg << 16);
 #pragma unroll
                     for (uint32_t t = 0; t < 5; ++t)  // at most five triangles a case
                         if (t < n) jobs[j + t] = job | (t << 12);
@@ -1097,13 +1100,14 @@ __device__ __forceinline__ void emit_block(const Problem &p, const WPlan &pl, un
                 const uint32_t jend = (q + 1 < BB) ? tp[q + 1] : nt;
                 if (j >= w1 || jend <= w0) continue;
                 uint32_t mm = mmk[q];
+                const uint32_t cell0 = VT ? (q + fdiv(q, pl.rB)) * pl.B1 : q * B;
                 while (mm) {
                     const uint32_t x = __ffs(mm) - 1;
                     mm &= mm - 1u;
                     const uint32_t cfg = ck[q * B + x];
                     const uint32_t n = ntab[cfg];
                     for (uint32_t t = 0; t < n; ++t, ++j)
-                        if (j >= w0 && j < w1) jobs[j - w0] = (q * B + x) | (t << 12) | (cfg << 16);
+                        if (j >= w0 && j < w1) jobs[j - w0] = (cell0 + x) | (t << 12) | (cfg << 16);
                 }
             }
         }
@@ -1114,17 +1118,17 @@ __device__ __forceinline__ void emit_block(const Problem &p, const WPlan &pl, un
             if (lane < n && MTX_BC(w0 + b + lane, nt, kBcIndex)) {
                 const uint32_t job = jobs[b + lane];
                 const uint32_t i = job & 0xfffu, t = (job >> 12) & 7u;
-                const uint32_t q = fdiv(i, pl.rB), x = i - q * B;
-                const uint32_t z = fdiv(q, pl.rB), y = q - z * B;
                 const uint64_t w = tab[job >> 16] >> (4 + 12 * t);
                 uint32_t *o = indices + 3ull * (tbase + w0 + b + lane);  // each lane its own 12 bytes
                 if constexpr (VT) {
-                    const uint32_t ti = (z * pl.B1 + y) * pl.B1 + x;
+                    const uint32_t ti = i;  // the cell's low corner in the vertex table
                     const uint16_t *eoff = reinterpret_cast<const uint16_t *>(owner + 16);  // edge_offsets
                     o[0] = edge_vertex_ut(ti, (uint32_t)(w & 0xFu), eoff, vt, um, nbase, pl.B1, bad);
                     o[1] = edge_vertex_ut(ti, (uint32_t)((w >> 4) & 0xFu), eoff, vt, um, nbase, pl.B1, bad);
                     o[2] = edge_vertex_ut(ti, (uint32_t)((w >> 8) & 0xFu), eoff, vt, um, nbase, pl.B1, bad);
                 } else {
+                    const uint32_t q = fdiv(i, pl.rB), x = i - q * B;
+                    const uint32_t z = fdiv(q, pl.rB), y = q - z * B;
                     o[0] = edge_vertex(x, y, z, (uint32_t)(w & 0xFu), owner, cross, vp, nvid, nm, B, BB,
                                        d.vertexOffset, bad);
                     o[1] = edge_vertex(x, y, z, (uint32_t)((w >> 4) & 0xFu), owner, cross, vp, nvid, nm, B, BB,
