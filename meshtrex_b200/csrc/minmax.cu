@@ -46,7 +46,7 @@ __global__ void __launch_bounds__(128) minmax_leaf_vec_kernel(const T *__restric
 constexpr int kTmaRows(int B) { return 4 * B + 1; }
 constexpr uint32_t kTmaMain(int B) { return (uint32_t)kTmaRows(B) * 512u; }
 constexpr uint32_t kTmaStage(int B) { return (kTmaMain(B) + 127u) / 128u * 128u; }
-constexpr int kTmaStages(int B) { return B == 4 ? 4 : 2; }  // about 35 KB per CTA at B = 4 and 8
+constexpr int kTmaStages(int B) { return B == 4 ? 4 : 2; }  // about 34 KB per CTA at B = 4 and 8
 constexpr int kTmaCtasPerSm = 4;  // 16 warps: enough to hide the fold's latencies, smem left for other kernels
 
 struct TmaLeafArgs {
