@@ -119,8 +119,8 @@ __host__ __device__ inline WPlan make_wplan(uint32_t B, uint32_t esz, bool tma, 
     if (tri_pass) {  // context first vertices: 16-bit packed entries for B <= 8 (gather_finish<CPL, true>)
         p.off_nvid = o;
         o = align_up(o + (B <= 8 ? 2 : 4) * p.nb3, 16);
-        p.off_nm = o;
-        o = align_up(o + p.nb3, 16);
+        p.off_nm = o;  // owned-edge masks (B > 8; packed into the entries for B <= 8)
+        if (B > 8) o = align_up(o + p.nb3, 16);
     }
     p.off_jobs = o;  // a window of packed jobs (triangles or vertices) in output order: the emit pass only
     if (tri_pass) o = align_up(o + 4 * kJobWin, 16);
@@ -745,13 +745,12 @@ __device__ __forceinline__ void build_utab(const WPlan &pl, unsigned char *ws, u
         }
     }
     const uint16_t *nvid = reinterpret_cast<const uint16_t *>(ws + pl.off_nvid);
-    const uint8_t *nm = ws + pl.off_nm;
     for (uint32_t j = lane; j < pl.nb3; j += 32) {
-        const uint32_t e = cmap[j];
+        const uint32_t e = cmap[j], v = nvid[j];
         const uint32_t ti = (((e >> 23) & 31u) * B1 + ((e >> 18) & 31u)) * B1 + ((e >> 13) & 31u);
         if (MTX_BC(ti, B1 * B1 * B1, kBcVoxTab)) {
-            ut[ti] = nvid[j];
-            um[ti] = nm[j];
+            ut[ti] = (uint16_t)((v & 0x7ffu) | ((e & 7u) << 11));
+            um[ti] = (uint8_t)(v >> 11);
         }
     }
     __syncwarp();
@@ -944,9 +943,10 @@ __device__ __forceinline__ void gather_issue_map(const Problem &p, const WPlan &
 // Turns the gathered records into first-vertex ids and owned-edge masks of the
 // context layer (nb_vb: lane c holds neighbour c's first vertex id).
 // PACKED (B <= 8, the unified table of build_utab): each entry keeps the
-// neighbour-relative first vertex and the neighbour's number, rel | c << 11,
-// and lanes 0-7 store the first vertex of the block (vbase, entry 0) and of
-// its neighbours into the plan's eight base words.
+// neighbour-relative first vertex and the voxel's owned-edge mask, rel | m <<
+// 11 (the neighbour's number comes from the context map), and lanes 0-7 store
+// the first vertex of the block (vbase, entry 0) and of its neighbours into
+// the plan's eight base words.
 template <int CPL, bool PACKED = false>
 __device__ __forceinline__ void gather_finish(const WPlan &pl, uint32_t nb_vb, const uint32_t rec[CPL],
                                               unsigned char *ws, uint32_t vbase = 0) {
@@ -964,11 +964,12 @@ __device__ __forceinline__ void gather_finish(const WPlan &pl, uint32_t nb_vb, c
         const uint32_t vb = PACKED ? 0u : __shfl_sync(0xffffffffu, nb_vb, (rec[k] >> 27) & 7u);
         if (j < nb3) {
             const bool present = rec[k] >> 31;
-            if constexpr (PACKED)
-                nvid16[j] = (uint16_t)((rec[k] & 0x7ffu) | (((rec[k] >> 27) & 7u) << 11));
-            else
+            if constexpr (PACKED) {
+                nvid16[j] = (uint16_t)((rec[k] & 0x7ffu) | (present ? ((rec[k] >> 24) & 7u) << 11 : 0u));
+            } else {
                 nvid[j] = present ? vb + (rec[k] & 0xffffffu) : kNoVertex;
-            nm[j] = present ? (uint8_t)((rec[k] >> 24) & 7u) : (uint8_t)0;
+                nm[j] = present ? (uint8_t)((rec[k] >> 24) & 7u) : (uint8_t)0;
+            }
         }
     }
 }
