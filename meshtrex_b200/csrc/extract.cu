@@ -114,9 +114,9 @@ __global__ void __launch_bounds__(kScanThreads)
 // CPL: context voxels per lane, ceil((3B^2 + 3B + 1) / 32): 8 covers B <= 8, 32 covers B <= 16.
 // The xyz form of B <= 8 is bounded to 85 registers (three CTAs of 256
 // threads); it uses 60 at the compile-time edge 8 and about 68 otherwise, with
-// no spills, so shared memory (28.4 KB a CTA of four warps for 8- and 16-bit
-// voxels) sets its seven CTAs an SM.  The other forms would spill under that
-// bound.
+// no spills; with 27.9 KB of shared memory a CTA of four warps (8- and 16-bit
+// voxels) eight CTAs share an SM at edge 8.  The other forms would spill
+// under that bound.
 template <typename T, int CPL, bool TMA, bool GENERIC, int BC>
 __global__ void __launch_bounds__(kMaxWarps * 32, (!GENERIC && CPL == 8) ? 3 : 1)
     pmb_emit_kernel(Problem p_, const __grid_constant__ CUtensorMap map, const uint32_t *__restrict__ ids,
