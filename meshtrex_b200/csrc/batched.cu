@@ -458,7 +458,7 @@ __device__ __forceinline__ void batch_count_block(const BatchArgs &a, const Prob
     count_block_balanced(p, pl, ws, g, ntab, a.desc + r, a.faces + (uint64_t)r * a.face_stride);
 }
 
-template <int CPL, bool GENERIC>
+template <int CPL, bool GENERIC, bool EO>
 __device__ __forceinline__ void batch_emit_block(const BatchArgs &a, const Problem &p, const WPlan &pl,
                                                  const GridDiv &dv, unsigned char *ws, const uint64_t *tab,
                                                  const uint8_t *ntab, const uint8_t *owner, uint32_t id, uint32_t r,
@@ -478,7 +478,7 @@ __device__ __forceinline__ void batch_emit_block(const BatchArgs &a, const Probl
     uint32_t rec[CPL];
     gather_issue<CPL, false>(p, pl, g, nb_rk, a.faces, a.face_stride, rec);
     fill_context_vertices<CPL>(pl, ws, nb_vb, rec);
-    emit_triangles_balanced(p, pl, ws, g, d, tab, ntab, owner, a.indices + jr.indexOffset, &a.ctrl->status, r);
+    emit_triangles_balanced<EO>(p, pl, ws, g, d, tab, ntab, owner, a.indices + jr.indexOffset, &a.ctrl->status, r);
 }
 
 // ------------------------------------------------------------ the kernel
@@ -505,6 +505,7 @@ __global__ void __launch_bounds__(kBThreads, BC ? 4 : 1) batch_extract_kernel(co
         ntab[i] = (uint8_t)(c_mc_cases[i] & 0xFu);
     }
     if (tid < 12) owner[tid] = c_mc_owner[tid];
+    if (BC) edge_offsets(reinterpret_cast<uint16_t *>(owner + 16), BC + 1);  // the edge is known: table_vertex<true>
     __syncthreads();
     BCtrl *ctrl = a.ctrl;
     DevStatus *st = &ctrl->status;
@@ -587,7 +588,7 @@ __global__ void __launch_bounds__(kBThreads, BC ? 4 : 1) batch_extract_kernel(co
             jr.indexOffset = __ldcg(&a.res[j].indexOffset);
             jr.vertexCount = __ldcg(&a.res[j].vertexCount);
             jr.indexCount = __ldcg(&a.res[j].indexCount);
-            batch_emit_block<CPL, GENERIC>(a, p, pl, v.dv, ws, tab, ntab, owner, id, r, job.rank_off, jr);
+            batch_emit_block<CPL, GENERIC, BC != 0>(a, p, pl, v.dv, ws, tab, ntab, owner, id, r, job.rank_off, jr);
         }
     }
 }

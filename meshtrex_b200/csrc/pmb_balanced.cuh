@@ -267,11 +267,22 @@ __device__ __forceinline__ void fill_own_vertices(const WPlan &pl, unsigned char
 
 // Vertex id of cube edge e of the cell at tile index c: the owner voxel
 // (c + dx + dy*B1 + dz*B1^2, owner byte dx | dy << 1 | dz << 2 | axis << 3)
-// and the owned edges of lower axes before it.
+// and the owned edges of lower axes before it.  EO: the CTA's edge-offset
+// table (edge_offsets, after the owner bytes) holds offset | axis << 8 for a
+// block edge known at compile time.
+template <bool EO = false>
 __device__ __forceinline__ uint32_t table_vertex(uint32_t c, uint32_t e, const uint8_t *owner, uint32_t B1,
                                                  const uint32_t *vtab, const uint8_t *vmsk, bool &bad) {
-    const uint32_t o = owner[e];
-    const uint32_t i = c + (o & 1u) + ((o >> 1) & 1u) * B1 + ((o >> 2) & 1u) * B1 * B1, ax = o >> 3;
+    uint32_t i, ax;
+    if constexpr (EO) {
+        const uint32_t eo = reinterpret_cast<const uint16_t *>(owner + 16)[e];
+        i = c + (eo & 0xffu);
+        ax = eo >> 8;
+    } else {
+        const uint32_t o = owner[e];
+        i = c + (o & 1u) + ((o >> 1) & 1u) * B1 + ((o >> 2) & 1u) * B1 * B1;
+        ax = o >> 3;
+    }
     const uint32_t m = vmsk[i];
     bad |= !((m >> ax) & 1u);
     return vtab[i] + __popc(m & ((1u << ax) - 1u));
@@ -313,6 +324,7 @@ __device__ __forceinline__ void resolve_vertices(const Problem &p, const WPlan &
 
 // Triangle jobs [done, done + n), n <= 32, one per lane: job = tile index of
 // the cell | t << 13 | case << 16; writes the n triangles from dst on.
+template <bool EO = false>
 __device__ __forceinline__ void resolve_triangles(const WPlan &pl, unsigned char *ws, const uint64_t *tab,
                                                   const uint8_t *owner, uint32_t done, uint32_t n, uint32_t *dst,
                                                   bool &bad) {
@@ -326,9 +338,9 @@ __device__ __forceinline__ void resolve_triangles(const WPlan &pl, unsigned char
         const uint32_t job = jobs[(done + lane) & (kRing - 1)];
         const uint32_t cell = job & 0x1fffu, t = (job >> 13) & 7u;
         const uint64_t w = tab[job >> 16] >> (4 + 12 * t);
-        dst[3 * lane + 0] = table_vertex(cell, (uint32_t)(w & 0xFu), owner, B1, vtab, vmsk, bad);
-        dst[3 * lane + 1] = table_vertex(cell, (uint32_t)((w >> 4) & 0xFu), owner, B1, vtab, vmsk, bad);
-        dst[3 * lane + 2] = table_vertex(cell, (uint32_t)((w >> 8) & 0xFu), owner, B1, vtab, vmsk, bad);
+        dst[3 * lane + 0] = table_vertex<EO>(cell, (uint32_t)(w & 0xFu), owner, B1, vtab, vmsk, bad);
+        dst[3 * lane + 1] = table_vertex<EO>(cell, (uint32_t)((w >> 4) & 0xFu), owner, B1, vtab, vmsk, bad);
+        dst[3 * lane + 2] = table_vertex<EO>(cell, (uint32_t)((w >> 8) & 0xFu), owner, B1, vtab, vmsk, bad);
     }
     __syncwarp();
 }
@@ -392,6 +404,7 @@ __device__ __forceinline__ bool emit_vertices_balanced(const Problem &p, const W
 
 // Second half: the block's own voxels into the vertex table, then its
 // triangles.
+template <bool EO = false>
 __device__ __forceinline__ void emit_triangles_balanced(const Problem &p, const WPlan &pl, unsigned char *ws,
                                                         const Geo &g, const mtx_meshlet_descriptor &d,
                                                         const uint64_t *tab, const uint8_t *ntab,
@@ -424,7 +437,7 @@ __device__ __forceinline__ void emit_triangles_balanced(const Problem &p, const 
         const uint32_t avail = min(top, nt);  // never write past the block's triangles
         while (avail - done >= (last ? 1u : 32u)) {
             const uint32_t n32 = min(32u, avail - done);
-            resolve_triangles(pl, ws, tab, owner, done, n32, indices + 3ull * (tbase + done), bad);
+            resolve_triangles<EO>(pl, ws, tab, owner, done, n32, indices + 3ull * (tbase + done), bad);
             done += n32;
         }
     }
