@@ -204,7 +204,7 @@ __device__ __forceinline__ void count_block_balanced(const Problem &p, const WPl
     uint32_t bnv, bnt;
     block_counts_balanced(p, pl, ws, g, ntab, true, bnv, bnt);
     if (lane == 0) *reinterpret_cast<uint2 *>(&dr->vertexCount) = make_uint2(bnv, bnt);
-    write_face_records(pl, ws, fr);
+    write_face_records<false>(pl, ws, fr);
 }
 
 // ---------------------------------------------------------- vertex table

@@ -977,13 +977,29 @@ __device__ __forceinline__ void gather_finish(const WPlan &pl, uint32_t nb_vb, c
 // The block's low-face records from its crossing rows and row prefixes:
 // block-relative first vertex | owned-edge mask << 24 of the voxels with
 // x == 0 (index z*B + y), y == 0 (BB + z*B + x) and z == 0 (2BB + y*B + x).
+// SPREAD: each y == 0 / z == 0 record computed by its own lane from its row's
+// prefix (coalesced stores; the single-volume count pass); otherwise 2B lanes
+// walk those rows along x with a running first vertex (the batched count phase).
+template <bool SPREAD = true>
 __device__ __forceinline__ void write_face_records(const WPlan &pl, const unsigned char *ws, uint32_t *fr) {
     const uint32_t lane = threadIdx.x & 31, B = pl.B, BB = pl.BB;
     const uint32_t *cross = reinterpret_cast<const uint32_t *>(ws + pl.off_cross);
     const uint32_t *vp = reinterpret_cast<const uint32_t *>(ws + pl.off_vp);
-    // y == 0 and z == 0 faces: lane l < 2B walks row (y = 0, z = l) or (y = l - B,
-    // z = 0) along x, the first vertex running up by each voxel's owned edges
-    if (lane < 2 * B) {
+    if constexpr (SPREAD) {
+        // records BB + i for i < 2BB: record i is voxel x of row q (y == 0:
+        // q = z*B; z == 0: q = y); consecutive lanes take consecutive records
+        for (uint32_t i = lane; i < 2 * BB; i += 32) {
+            const uint32_t face = i >= BB, rem = face ? i - BB : i;
+            const uint32_t r = fdiv(rem, pl.rB), x = rem - r * B;
+            const uint32_t q = face ? r : r * B;
+            const uint32_t xc = cross[q], yc = cross[BB + q], zc = cross[2 * BB + q];
+            const uint32_t below = (1u << x) - 1u;
+            const uint32_t run = vp[q] + __popc(xc & below) + __popc(yc & below) + __popc(zc & below);
+            const uint32_t m = ((xc >> x) & 1u) | (((yc >> x) & 1u) << 1) | (((zc >> x) & 1u) << 2);
+            if (MTX_BC(BB + i, 3 * BB, kBcFaces)) fr[BB + i] = run | (m << 24);
+        }
+    } else if (lane < 2 * B) {
+        // lane l < 2B walks row (y = 0, z = l) or (y = l - B, z = 0) along x
         const bool yface = lane < B;
         const uint32_t q = yface ? lane * B : lane - B;
         uint32_t *o = fr + (yface ? BB + lane * B : 2 * BB + (lane - B) * B);
