@@ -28,7 +28,7 @@ constexpr bool kSingleBuffer = true;
 // ------------------------------------------------------------- count pass
 // BC: the block edge at compile time (0: p.B at run time).  The bench's edge 8
 // has its own instantiation, in which the warp's shared-memory plan and every
-// division by the edge fold to constants (40 registers).  The run-time form is
+// division by the edge fold to constants (48 registers).  The run-time form is
 // held to 64 registers (no spills), where it would otherwise take up to 128.
 template <typename T, bool TMA, int BC>
 __global__ void __launch_bounds__(kMaxWarps * 32, BC ? 0 : 4)
